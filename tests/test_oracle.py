@@ -1,0 +1,165 @@
+"""The CPU oracle pinned against the reference's shipped results (golden
+fixtures) and, where oracle/_ref exists, against the reference binaries.
+No GPU needed."""
+import gzip
+import json
+import os
+import subprocess
+
+import pytest
+
+import oracle_lib as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def surv_lines(entry):
+    fn = os.path.join(GOLD, entry["survivors_file"])
+    op = gzip.open if fn.endswith(".gz") else open
+    with op(fn, "rt") as f:
+        return sorted(l.rstrip("\n") for l in f if l.strip())
+
+
+def run_entry(entry, X):
+    base = O.load_machine(entry["machine"])
+    if entry["mode"] == "delete":
+        r, job = O.setup(base, X, fmax=entry["fmax"])
+    else:
+        lo, hi = (entry["lo"], entry["hi"]) if entry["mode"] == "freesym" else (-1, -1)
+        r, job = O.setup(base, X, free_cells=entry["free"], lo=lo, hi=hi)
+    assert r >= 0
+    c, recs = O.search(job, nthreads=8)
+    return c, [O.survivor_line(X, rr, job.nq) for rr in recs]
+
+
+def check_counts(c, exp):
+    assert c["leaves"] == exp["leaves"]
+    assert c["survivors"] == exp["survivors"]
+    assert c["hist"] == exp["hist"]
+    if exp["steps"] is not None:
+        assert c["steps"] == exp["steps"]
+
+
+def test_keys_match_reference_targets():
+    k, t = O.keys()
+    assert len(k) == 1364 and t[0] == 0
+    # TGT[n] is the XOR of KEY over cells -1..2^n-2 (src/e13search.c:441-444)
+    for n in range(1, 10):
+        h = 0
+        for c in range(-1, (1 << n) - 1):
+            h ^= k[c + 64]
+        assert h == t[n]
+
+
+def test_base_erdos14():
+    base = O.load_machine("erdos_14.txt")
+    r = O.run_full(base, 14)
+    # base states=14 result=SURV stage=9 st0=2 head0=-2 abs=1 rel=0 steps=208864
+    line = open(os.path.join(GOLD, "base_erdos14.txt")).read().splitlines()[-1]
+    assert line == (f"base states=14 result={'SURV' if r[0] else 'DEAD'} stage={r[1]} st0={r[2]} head0={r[3]} "
+                    f"abs={r[4]} rel={r[5]} steps={r[6]}")
+
+
+def test_mutants():
+    base = O.load_machine("erdos_14.txt")
+    got = []
+    for i in range(28):
+        for v in range(-1, 56):
+            if v == base[i]:
+                continue
+            tab = list(base)
+            tab[i] = v
+            r = O.run_full(tab, 14)
+            got.append(f"{i} {v} {r[1]} {r[0]}")
+    exp = [l.rstrip("\n") for l in open(os.path.join(GOLD, "mutants.txt")) if l.strip() and not l.startswith("#")]
+    assert got == exp
+
+
+@pytest.mark.parametrize("name", ["local_edits_f2", "doubling_X0", "doubling_X1", "doubling_X2", "split_test",
+                                  "split_test_free"])
+def test_small_searches(searches, name):
+    e = searches[name]
+    xs = e["X"] if isinstance(e["X"], list) else [e["X"]]
+    lines = []
+    for X, exp in zip(xs, e["expect"]):
+        assert exp["X"] == X
+        c, l = run_entry(e, X)
+        check_counts(c, exp)
+        lines += l
+    if "survivors_file" in e:
+        assert sorted(lines) == surv_lines(e)
+
+
+@pytest.mark.parametrize("k", [1, 17, 61])
+def test_counters_f2(searches, k):
+    e = searches[f"counters_f2_base_{k:02d}"]
+    c, _ = run_entry(e, -1)
+    check_counts(c, e["expect"][0])
+
+
+def test_setup_errors():
+    base = O.load_machine("erdos_14.txt")
+    # X=2 has two forced cells: FMAX=1 skips it (src/e13search.c:353)
+    r, _ = O.setup(base, 2, fmax=1)
+    assert r == -1
+    # a fixed cell naming a symmetric state beyond the first unnamed one
+    r, _ = O.setup(base, 9, free_cells=["F0", "F1"], lo=3, hi=9)
+    assert r == -3
+    # start state inside the symmetric range
+    r, _ = O.setup(base, 13, free_cells=["A0", "A1"], lo=0, hi=13)
+    assert r in (-3, -4)
+
+
+def test_recheck_golden_first_v1_survivor():
+    lines = gzip.open(os.path.join(GOLD, "surv", "division_v1_1RD_fileorder.txt.gz"), "rt").read().splitlines()
+    v = json.load(gzip.open(os.path.join(GOLD, "recheck_1RD.json.gz"), "rt"))["verdicts"]
+    ok, verdict, _ = O.recheck_line(lines[0], 15)
+    assert verdict == v[0]
+
+
+def test_deep_golden():
+    for fn, survfn, nmax in (("deep_v2.txt", "division_v2_fileorder.txt", 16),):
+        exp = [l.rstrip("\n") for l in open(os.path.join(GOLD, "deep", fn)) if l.startswith("survivor")]
+        lines = open(os.path.join(GOLD, "surv", survfn)).read().splitlines()
+        # deep_v2 was run at some NMAX; take it from the longest line
+        n = max(int(tok[1:].split(":")[0]) for l in exp for tok in l.split() if tok.startswith("n") and ":" in tok)
+        for i, line in enumerate(lines[:2]):
+            got = f"survivor {i + 1} " + O.deep_line(line, n)
+            assert got == exp[i]
+
+
+REFBIN = os.path.join(O.REF_DIR, "e13search")
+
+
+@pytest.mark.skipif(not os.path.exists(REFBIN), reason="reference binaries not built here")
+@pytest.mark.parametrize("args", [
+    ["free", "erdos_14.txt", "5", "B0", "C1", "E0"],
+    ["freesym", "erdos_14.txt", "9", "3", "9", "H0", "H1", "I0", "I1"],
+    ["delete", "counters_3state/base_05.txt", "1", "-1"],
+    ["delete", "split_15.txt", "2", "3"],
+])
+def test_oracle_vs_reference_binary(args):
+    mode = args[0]
+    path = os.path.join(O.MACHINES, args[1])
+    r = subprocess.run([REFBIN, mode, path] + args[2:], capture_output=True, text=True, check=True,
+                       env=dict(os.environ, OMP_NUM_THREADS="4"))
+    ref = [O.parse_summary(l) for l in r.stderr.splitlines() if "leaves=" in l]
+    ref_surv = sorted(l for l in r.stdout.splitlines() if l.startswith("SURVIVOR"))
+    base = O.load_machine(args[1])
+    got_surv = []
+    if mode == "delete":
+        for X, exp in zip([int(x) for x in args[3:]], ref):
+            st, job = O.setup(base, X, fmax=int(args[2]))
+            c, recs = O.search(job)
+            check_counts(c, exp)
+            got_surv += [O.survivor_line(X, rr, job.nq) for rr in recs]
+    else:
+        X = int(args[2])
+        if mode == "freesym":
+            st, job = O.setup(base, X, free_cells=args[5:], lo=int(args[3]), hi=int(args[4]))
+        else:
+            st, job = O.setup(base, X, free_cells=args[3:])
+        c, recs = O.search(job)
+        check_counts(c, ref[0])
+        got_surv = [O.survivor_line(X, rr, job.nq) for rr in recs]
+    assert sorted(got_surv) == ref_surv
