@@ -1,0 +1,268 @@
+// e13_device.cuh -- device-side pieces shared by the search kernels, the
+// whole-table runner and the survivor checker of libe13b200.so (sm_100a).
+//
+// One Turing machine per lane.  A lane's tape (1364 cells, bit-packed into 43
+// words) and its table (16 rows of two 8-bit cell entries) live in shared
+// memory, interleaved by lane: word w of lane l sits at [w * blockDim + l], so
+// every lane always hits its own bank and a warp-wide access never conflicts.
+//
+// Semantics follow the reference's run() (src/e13search.c:134-177) step for
+// step: stage test, deadline, read, fork on a first read, halt, write + hash,
+// move, window bounds, state, t++.
+#pragma once
+#include <stdint.h>
+
+namespace e13dev {
+
+typedef unsigned long long u64;
+typedef unsigned int u32;
+
+constexpr int kTapeCells = 1364;  // cells -64 .. 1299 (src/e13search.c:59-61)
+constexpr int kTapeWords = 43;    // ceil(1364 / 32)
+constexpr int kLeft = 64;
+constexpr int kStages = 9;
+constexpr int kCounterCells = 62; // cells < -2 hash into the counter hash hc
+
+// Cell entry (one byte): 0..63 a move (the reference's code), plus flags.
+constexpr u32 kEntHalt = 0x40;    // halt
+constexpr u32 kEntUnread = 0x80;  // never read yet: the first read is an event
+constexpr u32 kEntFree = 0xFF;    // free cell, no move yet (FORCED, src/e13search.c:66)
+constexpr u32 kEntSpecial = 0xC0; // any of the above: leaves the fast path
+
+// Node flags byte.
+constexpr int kFlagAbs = 1, kFlagRel = 2, kFlagCs0 = 4, kFlagKeep = 32;
+
+// A machine stopped at a fork (pend = the cell being read for the first time)
+// or between slices (pend = -1, one child: go on).  Children still to run: the
+// keep child (kFlagKeep) and the alternatives in vmask (bit v = move v).
+struct __align__(16) Node {
+  u64 hb;             // hash of the ones at cells >= -2
+  u64 ch[3];          // counter hash at the first stage start with c = 0, 1, 2
+  u64 vmask;
+  int p, st, t, deadline;  // p = head + 64
+  signed char nt, stage, st0, flags;
+  short p0, pend;
+  unsigned char nintro, budget, pad0, pad1;
+  u32 pad2;
+  unsigned char ent[32];
+  u32 tape[kTapeWords];
+  u32 pad3;
+};
+static_assert(sizeof(Node) % 16 == 0, "Node must be a whole number of 16-byte chunks");
+constexpr int kNodeChunks = sizeof(Node) / 16;
+
+// Survivor record written by the device.
+struct SurvRec {
+  unsigned char ent[32];
+  int st0, head0, abs_ok, rel_ok, t, pad[3];
+};
+
+// Control block of one search (device memory).
+struct Ctl {
+  long long top;                 // nodes on the frontier stack
+  long long batch;               // this launch's input: stack[top - batch .. top)
+  unsigned long long cursor;     // input nodes taken
+  unsigned long long nout;       // nodes written to the output buffer
+  long long peak;
+  unsigned long long nsurv;      // survivors found (records kept: min(nsurv, cap))
+  int dump;                      // persistent: end the epoch now
+  int starved;                   // persistent: warps out of work
+  int error;                     // kErr* bits
+  int launches;
+  u64 leaves, steps;
+  u64 hist[kStages + 1];
+};
+constexpr int kErrOverflow = 1, kErrOutFull = 2;
+
+// The filter's constant tables (set by the host from e13_keys()).
+__constant__ u64 c_key[kTapeCells];
+__constant__ u64 c_tgt[kStages + 2];
+__constant__ int c_deadline[kStages + 2];  // 4 * erdos_14 stage step + 64 (src/e13search.c:159)
+__constant__ int c_exc[kStages + 1];       // exceptions by stage (src/e13search.c:71)
+
+enum { kEvRun = 0, kEvDead = 1, kEvSurv = 2, kEvStage = 3, kEvCell = 4 };
+
+// Registers of one lane's machine.
+struct Lane {
+  int p, st, t, deadline, tseg;
+  u64 hb, tgt;
+  int nt, stage, st0, p0, flags;
+  u64 ch0, ch1, ch2;
+  int nintro, budget;
+};
+
+__device__ __forceinline__ void tape_extent(int t, int &lo, int &hi) {
+  // After t steps from the blank tape the head has stayed within 64 +- t, so
+  // no other tape word can be nonzero.
+  int a = kLeft - t, b = kLeft + t;
+  a = a < 0 ? 0 : a;
+  b = b > kTapeCells - 1 ? kTapeCells - 1 : b;
+  lo = a >> 5;
+  hi = b >> 5;
+}
+
+// Runs up to n steps.  Returns kEvRun when n is used up, else the event that
+// stopped it; the lane is then exactly at the reference's state for that event.
+// The stage test of the current configuration has already been done on entry
+// (re-running it at the same configuration changes nothing, as the reference
+// notes at src/e13search.c:131-133).
+__device__ __forceinline__ int step_slice(int &p, int &st, int &t, const int deadline, u64 &hb, const u64 tgt,
+                                          u32 *__restrict__ tcol, const u32 *__restrict__ rcol,
+                                          const u64 *__restrict__ keyb, const int stride, int &n, int &cell) {
+  while (n > 0) {
+    if (t > deadline) return kEvDead;
+    const int widx = (p >> 5) * stride;
+    const u32 word = tcol[widx];
+    const u32 row = rcol[st * stride];
+    const u32 sym = (word >> (p & 31)) & 1u;
+    const u32 e = (row >> (sym << 4)) & 0xFFu;
+    if (e & kEntSpecial) {
+      cell = (st << 1) | (int)sym;
+      return kEvCell;
+    }
+    if ((e ^ sym) & 1u) {
+      tcol[widx] = word ^ (1u << (p & 31));
+      hb ^= keyb[p];  // zero for cells < -2: those go to the counter hash
+    }
+    p += (int)(e & 2u) - 1;
+    if ((unsigned)(p - 1) >= (unsigned)(kTapeCells - 2)) return kEvDead;  // head <= -64 or >= 1299
+    st = (int)(e >> 2);
+    ++t;
+    --n;
+    if (hb == tgt) return kEvStage;
+  }
+  return kEvRun;
+}
+
+// Counter hash from the tape: XOR of the keys of the ones at cells < -2
+// (exactly what the reference accumulates in hc, src/e13search.c:170).
+__device__ __forceinline__ u64 counter_hash(const u32 *tcol, const u64 *keyc, int stride) {
+  u64 hc = 0;
+  u32 w0 = tcol[0], w1 = tcol[stride] & 0x3FFFFFFFu;
+  while (w0) {
+    hc ^= keyc[__ffs(w0) - 1];
+    w0 &= w0 - 1;
+  }
+  while (w1) {
+    hc ^= keyc[31 + __ffs(w1)];
+    w1 &= w1 - 1;
+  }
+  return hc;
+}
+
+// The stage-start test of src/e13search.c:136-161 once hb matches TGT[nt].
+// Returns 0 (go on), kEvDead or kEvSurv.
+__device__ __forceinline__ int stage_check(Lane &L, const u32 *tcol, const u64 *keyc, int stride) {
+  const int nt = L.nt, c = c_exc[nt];
+  int a = L.flags & kFlagAbs, r = (L.flags >> 1) & 1;
+  if (nt > 1) {
+    if (L.st != L.st0) return 0;
+    if (L.p != L.p0) a = 0;
+    if (L.p - (1 << nt) != L.p0 - 2) r = 0;
+    if (!a && !r) return 0;
+  }
+  const u64 hc = counter_hash(tcol, keyc, stride);
+  const u64 chc = c == 0 ? L.ch0 : (c == 1 ? L.ch1 : L.ch2);
+  if (((L.flags >> (2 + c)) & 1) && chc != hc) return kEvDead;
+  if (c != 0 && (L.flags & 4) && L.ch0 == hc) return kEvDead;
+  if (c != 1 && (L.flags & 8) && L.ch1 == hc) return kEvDead;
+  if (c != 2 && (L.flags & 16) && L.ch2 == hc) return kEvDead;
+  L.flags |= kFlagCs0 << c;
+  if (c == 0) L.ch0 = hc;
+  else if (c == 1) L.ch1 = hc;
+  else L.ch2 = hc;
+  if (nt == 1) {
+    L.st0 = L.st;
+    L.p0 = L.p;
+  }
+  L.flags = (L.flags & ~3) | a | (r << 1);
+  L.stage = nt;
+  if (nt == kStages) return kEvSurv;
+  L.nt = nt + 1;
+  L.deadline = c_deadline[nt + 1];
+  L.tgt = c_tgt[nt + 1];
+  return 0;
+}
+
+__device__ __forceinline__ u32 get_entry(const u32 *rcol, int stride, int cell) {
+  return (rcol[(cell >> 1) * stride] >> ((cell & 1) << 4)) & 0xFFu;
+}
+
+__device__ __forceinline__ void set_entry(u32 *rcol, int stride, int cell, u32 v) {
+  u32 *w = rcol + (cell >> 1) * stride;
+  const int sh = (cell & 1) << 4;
+  *w = (*w & ~(0xFFu << sh)) | (v << sh);
+}
+
+// Relabel symmetry (src/e13search.c:206-212): states in use after move v, or
+// -1 when v names a symmetric state past the next unused one.
+__device__ __forceinline__ int sym_after(int v, int nintro, int sym_lo, int sym_hi) {
+  if (sym_lo < 0 || v < 0) return nintro;
+  const int q = v >> 2;
+  if (q < sym_lo || q > sym_hi) return nintro;
+  if (q - sym_lo < nintro) return nintro;
+  return (q - sym_lo == nintro) ? nintro + 1 : -1;
+}
+
+// Children of a first read of a cell with entry e (src/e13search.c:221-251):
+// keep the table's move unless the cell is free; while the cell is free or
+// budget remains, every other move the symmetry rule allows.
+__device__ __forceinline__ void child_set(u32 e, int budget, int nintro, int nv, int sym_lo, int sym_hi, int &keep,
+                                          u64 &vm) {
+  const bool is_free = (e == kEntFree);
+  keep = is_free ? 0 : 1;
+  vm = 0;
+  if (is_free || budget > 0) {
+    vm = nv >= 64 ? ~0ull : ((1ull << nv) - 1ull);
+    if (!is_free && !(e & kEntHalt)) vm &= ~(1ull << (e & 0x3Fu));
+    if (sym_lo >= 0) {
+      const int q0 = sym_lo + nintro + 1;  // first state a move may not name yet
+      if (q0 <= sym_hi) {
+        const int a = 4 * q0, b = 4 * (sym_hi + 1);
+        const u64 below_b = b >= 64 ? ~0ull : ((1ull << b) - 1ull);
+        const u64 below_a = (1ull << a) - 1ull;
+        vm &= ~(below_b & ~below_a);
+      }
+    }
+  }
+}
+
+// Position of the r-th (0-based) set bit of m (r < popc(m)).
+__device__ __forceinline__ int nth_bit64(u64 m, int r) {
+  u32 x = (u32)m;
+  int base = 0;
+  const int nlo = __popc(x);
+  if (r >= nlo) {
+    r -= nlo;
+    x = (u32)(m >> 32);
+    base = 32;
+  }
+  int c = __popc(x & 0xFFFFu);
+  if (r >= c) { r -= c; x >>= 16; base += 16; }
+  c = __popc(x & 0xFFu);
+  if (r >= c) { r -= c; x >>= 8; base += 8; }
+  c = __popc(x & 0xFu);
+  if (r >= c) { r -= c; x >>= 4; base += 4; }
+  c = __popc(x & 0x3u);
+  if (r >= c) { r -= c; x >>= 2; base += 2; }
+  if (r >= (int)(x & 1u)) base += 1;
+  return base;
+}
+
+// Drops the first k children (keep first, then the lowest moves).
+__device__ __forceinline__ void drop_children(int &keep, u64 &vm, int k) {
+  if (k <= 0) return;
+  if (keep) {
+    keep = 0;
+    --k;
+  }
+  if (k <= 0) return;
+  if (k >= __popcll(vm)) {
+    vm = 0;
+    return;
+  }
+  const int b = nth_bit64(vm, k);
+  vm &= ~((1ull << b) - 1ull);
+}
+
+}  // namespace e13dev

@@ -1,0 +1,882 @@
+// e13_search.cu -- the TNF enumeration search on one B200 (sm_100a).
+//
+// Two kernels share one template:
+//
+//  * plain (PERSIST = false): one launch per frontier batch.  Each warp pulls
+//    frontier nodes and hands their children to idle lanes; a lane runs its
+//    child to the next fork, leaf or step cap.  Every fork goes back to the
+//    frontier.  The host waits for each launch (the reference GPU design,
+//    src/e13gpu.py:381-436, built B200-first).
+//
+//  * persistent (PERSIST = true): each warp runs a private depth-first search
+//    over the subtrees it pulls.  A forking lane pushes its node on the warp's
+//    stack and goes on with the first child in place (no copy); idle lanes take
+//    the next children of the stack top at the next round.  An epoch ends when
+//    enough warps starve or a time bound passes: warps then dump live lanes and
+//    stack nodes back to the frontier, and the next epoch rebalances.  Epochs
+//    are replayed from a captured CUDA graph; the host reads the control block
+//    once per graph.
+//
+// Leaves, steps and deaths per stage are exact and equal the reference's
+// (src/e13search.c:214-254 explore, :357-420 run_delete).
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "e13.h"
+#include "e13_device.cuh"
+
+using namespace e13dev;
+
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr int kMaxBlock = 896;
+constexpr int kKeySmemBytes = (kTapeCells + 64) * 8;
+
+// steps a lane gets between warp-level refill rounds is Params::slice
+
+struct Params {
+  int nq, nv, sym_lo, sym_hi;
+  int slice, step_cap, wdepth, starve_limit;
+  long long out_cap, out_soft, surv_cap;
+  long long epoch_ns;
+  Node *stack, *out, *wstack;
+  SurvRec *surv;
+  Ctl *ctl;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void lane_load(Lane &L, const Node *N, u32 *tcol, u32 *rcol, int stride, int nq) {
+  // clear what the previous machine of this lane may have written
+  int lo, hi;
+  tape_extent(L.t, lo, hi);
+  for (int w = lo; w <= hi; ++w) tcol[w * stride] = 0;
+  L.p = N->p;
+  L.st = N->st;
+  L.t = N->t;
+  L.deadline = N->deadline;
+  L.hb = N->hb;
+  L.nt = N->nt;
+  L.stage = N->stage;
+  L.st0 = N->st0;
+  L.p0 = N->p0;
+  L.flags = N->flags & 31;
+  L.ch0 = N->ch[0];
+  L.ch1 = N->ch[1];
+  L.ch2 = N->ch[2];
+  L.nintro = N->nintro;
+  L.budget = N->budget;
+  L.tgt = c_tgt[L.nt];
+  L.tseg = L.t;
+  const u32 *e32 = reinterpret_cast<const u32 *>(N->ent);
+  for (int k = 0; 2 * k < nq; ++k) {
+    const u32 w = e32[k];
+    rcol[(2 * k) * stride] = __byte_perm(w, 0u, 0x4140);
+    rcol[(2 * k + 1) * stride] = __byte_perm(w, 0u, 0x4342);
+  }
+  tape_extent(L.t, lo, hi);
+  for (int w = lo; w <= hi; ++w) tcol[w * stride] = N->tape[w];
+}
+
+__device__ __forceinline__ void lane_store(const Lane &L, Node *N, const u32 *tcol, const u32 *rcol, int stride,
+                                           int nq, int pend, int keep, u64 vm) {
+  N->hb = L.hb;
+  N->ch[0] = L.ch0;
+  N->ch[1] = L.ch1;
+  N->ch[2] = L.ch2;
+  N->vmask = vm;
+  N->p = L.p;
+  N->st = L.st;
+  N->t = L.t;
+  N->deadline = L.deadline;
+  N->nt = (signed char)L.nt;
+  N->stage = (signed char)L.stage;
+  N->st0 = (signed char)L.st0;
+  N->flags = (signed char)(L.flags | (keep ? kFlagKeep : 0));
+  N->p0 = (short)L.p0;
+  N->pend = (short)pend;
+  N->nintro = (unsigned char)L.nintro;
+  N->budget = (unsigned char)L.budget;
+  u32 *e32 = reinterpret_cast<u32 *>(N->ent);
+  for (int k = 0; 2 * k < nq; ++k) {
+    const u32 r0 = rcol[(2 * k) * stride];
+    const u32 r1 = (2 * k + 1 < 16) ? rcol[(2 * k + 1) * stride] : 0u;
+    e32[k] = __byte_perm(r0, r1, 0x6420);
+  }
+  int lo, hi;
+  tape_extent(L.t, lo, hi);
+  for (int w = lo; w <= hi; ++w) N->tape[w] = tcol[w * stride];
+}
+
+// Applies child `ch` (-1: keep / go on, else move v) of node N to a lane that
+// has just loaded N.
+__device__ __forceinline__ void apply_child(Lane &L, const Node *N, int ch, u32 *rcol, int stride, int sym_lo,
+                                            int sym_hi) {
+  const int pend = N->pend;
+  if (pend < 0) return;
+  const u32 e = N->ent[pend];
+  if (ch < 0) {
+    set_entry(rcol, stride, pend, e & 0x7Fu);  // the table's own move (or halt), now read
+  } else {
+    if (e != kEntFree) L.budget -= 1;
+    L.nintro = sym_after(ch, L.nintro, sym_lo, sym_hi);
+    set_entry(rcol, stride, pend, (u32)ch);
+  }
+}
+
+__device__ __forceinline__ void copy_node(Node *dst, const Node *src, int lane) {
+  if (lane < kNodeChunks) reinterpret_cast<uint4 *>(dst)[lane] = reinterpret_cast<const uint4 *>(src)[lane];
+}
+
+__device__ __forceinline__ void record_survivor(const Params &P, const Lane &L, const u32 *rcol, int stride) {
+  const unsigned long long k = atomicAdd(&P.ctl->nsurv, 1ull);
+  if ((long long)k >= P.surv_cap) return;
+  SurvRec *r = P.surv + k;
+  u32 *e32 = reinterpret_cast<u32 *>(r->ent);
+  for (int k2 = 0; k2 < 8; ++k2) {
+    const u32 r0 = (2 * k2 < P.nq) ? rcol[(2 * k2) * stride] : 0xC0C0u;
+    const u32 r1 = (2 * k2 + 1 < P.nq) ? rcol[(2 * k2 + 1) * stride] : 0xC0C0u;
+    e32[k2] = __byte_perm(r0, r1, 0x6420);
+  }
+  r->st0 = L.st0;
+  r->head0 = L.p0 - kLeft;
+  r->abs_ok = L.flags & 1;
+  r->rel_ok = (L.flags >> 1) & 1;
+  r->t = L.t;
+}
+
+enum { kStRun = 0, kStIdle = 1, kStFork = 2, kStCap = 3 };
+
+template <bool PERSIST>
+__global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  u64 *keyb = reinterpret_cast<u64 *>(smem_raw);  // keys of cells >= -2 (0 below)
+  u64 *keyc = keyb + kTapeCells;                  // keys of cells < -2
+  u32 *tape = reinterpret_cast<u32 *>(keyc + 64);
+  const int stride = blockDim.x;
+  u32 *rows = tape + kTapeWords * stride;
+  __shared__ unsigned long long s_hist[kStages + 1];
+  __shared__ unsigned long long s_leaves, s_steps;
+
+  for (int i = threadIdx.x; i < kTapeCells; i += stride) keyb[i] = (i >= kCounterCells) ? c_key[i] : 0ull;
+  for (int i = threadIdx.x; i < 64; i += stride) keyc[i] = (i < kCounterCells) ? c_key[i] : 0ull;
+  if (threadIdx.x <= kStages) s_hist[threadIdx.x] = 0;
+  if (threadIdx.x == 0) {
+    s_leaves = 0;
+    s_steps = 0;
+  }
+  u32 *tcol = tape + threadIdx.x;
+  u32 *rcol = rows + threadIdx.x;
+  for (int w = 0; w < kTapeWords; ++w) tcol[w * stride] = 0;
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const long long gwarp = ((long long)blockIdx.x * stride + threadIdx.x) >> 5;
+  Ctl *ctl = P.ctl;
+  const long long top0 = ctl->top;
+  const long long batch = ctl->batch;
+  Node *wst = PERSIST ? P.wstack + gwarp * P.wdepth : nullptr;
+  const unsigned long long t_begin = PERSIST ? globaltimer() : 0ull;
+
+  Lane L;
+  L.t = 0;
+  L.tseg = 0;
+  int status = kStIdle;
+  int fork_cell = 0;
+  u32 fork_e = 0;
+  unsigned leaves = 0;
+  unsigned long long steps = 0;
+
+  // warp-uniform state
+  int sp = 0;                  // persistent: nodes on this warp's stack
+  bool have_cur = false;       // a node whose children are being handed out
+  const Node *cur = nullptr;   // plain: that node (in the input)
+  int cur_keep = 0;
+  u64 cur_vm = 0;
+  bool input_done = false;
+  bool counted_starve = false;
+  int rounds = 0;              // slices run: a warp dumps only after one (progress every epoch)
+
+  for (;;) {
+    // ---- (A) forks
+    if (__any_sync(kFull, status == kStFork)) {
+      int keep = 0;
+      u64 vm = 0;
+      if (status == kStFork) child_set(fork_e, L.budget, L.nintro, P.nv, P.sym_lo, P.sym_hi, keep, vm);
+      if (PERSIST) {
+        // the forking lane goes on with the first child; the rest is pushed
+        int first = -2;
+        if (status == kStFork) {
+          if (keep) {
+            first = -1;
+            keep = 0;
+          } else {
+            first = __ffsll((long long)vm) - 1;
+            vm &= vm - 1;
+          }
+        }
+        const bool more = (status == kStFork) && (keep || vm);
+        const unsigned pm = __ballot_sync(kFull, more);
+        if (pm) {
+          if (have_cur && sp > 0 && lane == 0) {
+            wst[sp - 1].vmask = cur_vm;
+            wst[sp - 1].flags = (signed char)((wst[sp - 1].flags & 31) | (cur_keep ? kFlagKeep : 0));
+          }
+          __syncwarp();
+          const int rank = __popc(pm & lt_mask);
+          const int npush = min(__popc(pm), P.wdepth - sp);
+          if (more) {
+            Node *dst = nullptr;
+            if (rank < npush) {
+              dst = wst + sp + rank;
+            } else {
+              const unsigned long long k = atomicAdd(&ctl->nout, 1ull);
+              if ((long long)k < P.out_cap) dst = P.out + k;
+              else atomicOr(&ctl->error, kErrOutFull);
+            }
+            if (dst) lane_store(L, dst, tcol, rcol, stride, P.nq, fork_cell, keep, vm);
+          }
+          if (npush > 0) {
+            const int src = nth_bit64((u64)pm, npush - 1);  // lane holding the last node pushed on the warp stack
+            cur_keep = __shfl_sync(kFull, keep, src);
+            const unsigned lo = __shfl_sync(kFull, (unsigned)vm, src);
+            const unsigned hi = __shfl_sync(kFull, (unsigned)(vm >> 32), src);
+            cur_vm = ((u64)hi << 32) | lo;
+            sp += npush;
+            have_cur = true;
+          }
+          __syncwarp();
+        }
+        if (status == kStFork) {
+          // the fork's own state becomes its first child, in place
+          if (first < 0) {
+            set_entry(rcol, stride, fork_cell, fork_e & 0x7Fu);
+          } else {
+            if (fork_e != kEntFree) L.budget -= 1;
+            L.nintro = sym_after(first, L.nintro, P.sym_lo, P.sym_hi);
+            set_entry(rcol, stride, fork_cell, (u32)first);
+          }
+          status = kStRun;
+        }
+      } else {
+        if (status == kStFork) {
+          const unsigned long long k = atomicAdd(&ctl->nout, 1ull);
+          if ((long long)k < P.out_cap) lane_store(L, P.out + k, tcol, rcol, stride, P.nq, fork_cell, keep, vm);
+          else atomicOr(&ctl->error, kErrOutFull);
+          status = kStIdle;
+        }
+      }
+    }
+    if (!PERSIST && __any_sync(kFull, status == kStCap)) {
+      if (status == kStCap) {
+        const unsigned long long k = atomicAdd(&ctl->nout, 1ull);
+        if ((long long)k < P.out_cap) lane_store(L, P.out + k, tcol, rcol, stride, P.nq, -1, 1, 0ull);
+        else atomicOr(&ctl->error, kErrOutFull);
+        status = kStIdle;
+      }
+    }
+
+    // ---- (B) refill idle lanes
+    for (;;) {
+      const unsigned im = __ballot_sync(kFull, status == kStIdle);
+      if (!im) break;
+      if (!have_cur) {
+        if (PERSIST && sp > 0) {
+          const Node *N = wst + sp - 1;
+          cur_keep = (N->flags & kFlagKeep) ? 1 : 0;
+          cur_vm = N->vmask;
+          have_cur = true;
+        } else {
+          if (input_done) break;
+          long long k = batch;
+          // once an epoch is ending, leave the rest of the input where it is
+          if (lane == 0 && !(PERSIST && *((volatile int *)&ctl->dump)))
+            k = (long long)atomicAdd(&ctl->cursor, 1ull);
+          k = __shfl_sync(kFull, k, 0);
+          if (k >= batch) {
+            input_done = true;
+            break;
+          }
+          const Node *src = P.stack + (top0 - 1 - k);
+          if (PERSIST) {
+            copy_node(wst, src, lane);
+            __syncwarp();
+            sp = 1;
+          } else {
+            cur = src;
+          }
+          cur_keep = (src->flags & kFlagKeep) ? 1 : 0;
+          cur_vm = src->vmask;
+          have_cur = true;
+        }
+      }
+      const Node *N = PERSIST ? (wst + sp - 1) : cur;
+      const int navail = cur_keep + __popcll(cur_vm);
+      const int nidle = __popc(im);
+      const int rank = __popc(im & lt_mask);
+      if (status == kStIdle && rank < navail) {
+        int ch = -1;
+        if (!(cur_keep && rank == 0)) ch = nth_bit64(cur_vm, rank - cur_keep);
+        lane_load(L, N, tcol, rcol, stride, P.nq);
+        apply_child(L, N, ch, rcol, stride, P.sym_lo, P.sym_hi);
+        status = kStRun;
+      }
+      __syncwarp();
+      if (nidle >= navail) {
+        have_cur = false;
+        if (PERSIST) --sp;
+      } else {
+        drop_children(cur_keep, cur_vm, nidle);
+      }
+    }
+
+    // ---- (C) end of work / end of epoch
+    const bool any_run = __any_sync(kFull, status == kStRun);
+    if (!any_run && input_done && !have_cur && (!PERSIST || sp == 0)) {
+      if (PERSIST && lane == 0 && !counted_starve) atomicAdd(&ctl->starved, 1);
+      break;
+    }
+    if (PERSIST) {
+      int d = 0;
+      if (lane == 0) {
+        d = *((volatile int *)&ctl->dump);
+        if (!d && globaltimer() - t_begin > (unsigned long long)P.epoch_ns) d = 1;
+        if (!d && *((volatile int *)&ctl->starved) >= P.starve_limit) d = 1;
+        if (!d && (long long)*((volatile unsigned long long *)&ctl->nout) > P.out_soft) d = 1;
+        if (d) *((volatile int *)&ctl->dump) = 1;
+      }
+      d = __shfl_sync(kFull, d, 0);
+      if (!d && input_done && sp == 0 && !have_cur && !counted_starve) {
+        const int nidle = __popc(__ballot_sync(kFull, status == kStIdle));
+        if (nidle >= 16) {
+          if (lane == 0) atomicAdd(&ctl->starved, 1);
+          counted_starve = true;
+        }
+      }
+      if (d && rounds > 0) {
+        // dump: live lanes as resume nodes, then this warp's stack
+        if (status == kStRun) {
+          steps += (unsigned long long)(L.t - L.tseg);
+          L.tseg = L.t;
+          const unsigned long long k = atomicAdd(&ctl->nout, 1ull);
+          if ((long long)k < P.out_cap) lane_store(L, P.out + k, tcol, rcol, stride, P.nq, -1, 1, 0ull);
+          else atomicOr(&ctl->error, kErrOutFull);
+          status = kStIdle;
+        }
+        if (have_cur && sp > 0 && lane == 0) {
+          wst[sp - 1].vmask = cur_vm;
+          wst[sp - 1].flags = (signed char)((wst[sp - 1].flags & 31) | (cur_keep ? kFlagKeep : 0));
+        }
+        __syncwarp();
+        if (sp > 0) {
+          unsigned long long base = 0;
+          if (lane == 0) base = atomicAdd(&ctl->nout, (unsigned long long)sp);
+          base = __shfl_sync(kFull, base, 0);
+          for (int i = 0; i < sp; ++i) {
+            if ((long long)(base + i) < P.out_cap) copy_node(P.out + base + i, wst + i, lane);
+            else if (lane == 0) atomicOr(&ctl->error, kErrOutFull);
+          }
+        }
+        break;
+      }
+    }
+
+    // ---- (D) run a slice
+    ++rounds;
+    if (status == kStRun) {
+      int n = P.slice;
+      for (;;) {
+        int cell = 0;
+        int ev = step_slice(L.p, L.st, L.t, L.deadline, L.hb, L.tgt, tcol, rcol, keyb, stride, n, cell);
+        if (ev == kEvRun) break;
+        if (ev == kEvStage) {
+          ev = stage_check(L, tcol, keyc, stride);
+          if (ev == 0) {
+            if (n > 0) continue;
+            break;
+          }
+        } else if (ev == kEvCell) {
+          const u32 e = get_entry(rcol, stride, cell);
+          if (e == kEntHalt) {
+            ev = kEvDead;
+          } else if (e == kEntFree || L.budget > 0) {
+            steps += (unsigned long long)(L.t - L.tseg);
+            L.tseg = L.t;
+            fork_cell = cell;
+            fork_e = e;
+            status = kStFork;
+            break;
+          } else {
+            // first read with nothing to branch on: the cell is now fixed
+            set_entry(rcol, stride, cell, e & 0x7Fu);
+            if ((e & 0x7Fu) == kEntHalt) ev = kEvDead;
+            else continue;
+          }
+        }
+        // a leaf
+        steps += (unsigned long long)(L.t - L.tseg);
+        L.tseg = L.t;
+        ++leaves;
+        if (ev == kEvDead) {
+          atomicAdd(&s_hist[L.stage], 1ull);
+        } else {
+          record_survivor(P, L, rcol, stride);
+        }
+        status = kStIdle;
+        break;
+      }
+      if (!PERSIST && status == kStRun && L.t - L.tseg >= P.step_cap) {
+        steps += (unsigned long long)(L.t - L.tseg);
+        L.tseg = L.t;
+        status = kStCap;
+      }
+    }
+  }
+
+  // ---- totals
+  unsigned long long wl = leaves, ws = steps;
+  for (int o = 16; o > 0; o >>= 1) {
+    wl += __shfl_down_sync(kFull, wl, o);
+    ws += __shfl_down_sync(kFull, ws, o);
+  }
+  if (lane == 0) {
+    atomicAdd(&s_leaves, wl);
+    atomicAdd(&s_steps, ws);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicAdd(&ctl->leaves, s_leaves);
+    atomicAdd(&ctl->steps, s_steps);
+  }
+  if (threadIdx.x <= kStages && s_hist[threadIdx.x]) atomicAdd(&ctl->hist[threadIdx.x], s_hist[threadIdx.x]);
+}
+
+// Between launches: the input taken from the top of the stack is gone; the
+// outputs go where it was.
+__global__ void move_outputs(Ctl *ctl, Node *stack, const Node *out) {
+  const long long used = min((long long)ctl->cursor, ctl->batch);
+  const long long base = ctl->top - used;
+  const long long n = (long long)ctl->nout;
+  const long long chunks = n * kNodeChunks;
+  uint4 *dst = reinterpret_cast<uint4 *>(stack + base);
+  const uint4 *src = reinterpret_cast<const uint4 *>(out);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < chunks; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+__global__ void finish_launch(Ctl *ctl, long long cap, long long batch_max) {
+  const long long used = min((long long)ctl->cursor, ctl->batch);
+  long long top = ctl->top - used + (long long)ctl->nout;
+  ctl->top = top;
+  if (top > ctl->peak) ctl->peak = top;
+  ctl->batch = min(top, batch_max);
+  ctl->cursor = 0;
+  ctl->nout = 0;
+  ctl->dump = 0;
+  ctl->starved = 0;
+  ctl->launches += 1;
+}
+
+// Whole-table runs (src/e13search.c:428-433): one machine per thread.
+__global__ void __launch_bounds__(256) run_full_kernel(const int *tabs, int n, int nq, long long *out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  u64 *keyb = reinterpret_cast<u64 *>(smem_raw);
+  u64 *keyc = keyb + kTapeCells;
+  u32 *tape = reinterpret_cast<u32 *>(keyc + 64);
+  const int stride = blockDim.x;
+  u32 *rows = tape + kTapeWords * stride;
+  for (int i = threadIdx.x; i < kTapeCells; i += stride) keyb[i] = (i >= kCounterCells) ? c_key[i] : 0ull;
+  for (int i = threadIdx.x; i < 64; i += stride) keyc[i] = (i < kCounterCells) ? c_key[i] : 0ull;
+  __syncthreads();
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  u32 *tcol = tape + threadIdx.x;
+  u32 *rcol = rows + threadIdx.x;
+  for (int w = 0; w < kTapeWords; ++w) tcol[w * stride] = 0;
+  const int *tab = tabs + (long long)m * E13_MAXCELLS;
+  for (int s = 0; s < 16; ++s) {
+    u32 e0 = kEntHalt, e1 = kEntHalt;
+    if (s < nq) {
+      e0 = tab[2 * s] < 0 ? kEntHalt : (u32)tab[2 * s];
+      e1 = tab[2 * s + 1] < 0 ? kEntHalt : (u32)tab[2 * s + 1];
+    }
+    rcol[s * stride] = e0 | (e1 << 16);
+  }
+  Lane L;
+  L.p = kLeft; L.st = 0; L.t = 0; L.deadline = c_deadline[1]; L.hb = 0; L.tgt = c_tgt[1];
+  L.nt = 1; L.stage = 0; L.st0 = -1; L.p0 = 0; L.flags = 3; L.ch0 = L.ch1 = L.ch2 = 0;
+  int ev;
+  for (;;) {
+    int nn = 1 << 30, cell = 0;
+    ev = step_slice(L.p, L.st, L.t, L.deadline, L.hb, L.tgt, tcol, rcol, keyb, stride, nn, cell);
+    if (ev == kEvStage) {
+      ev = stage_check(L, tcol, keyc, stride);
+      if (ev == 0) continue;
+    }
+    if (ev == kEvCell) ev = kEvDead;  // only halts are special here
+    break;
+  }
+  long long *o = out + 7LL * m;
+  o[0] = ev == kEvSurv;
+  o[1] = L.stage;
+  o[2] = L.st0;
+  o[3] = L.p0 - kLeft;
+  o[4] = L.flags & 1;
+  o[5] = (L.flags >> 1) & 1;
+  o[6] = L.t;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------
+// host side
+
+struct e13_ctx {
+  int device;
+  int nsm;
+  cudaStream_t stream;
+  cudaEvent_t ev0, ev1, k0, k1;
+  bool consts_ready;
+  // buffers, grown on demand
+  Node *stack;
+  long long stack_cap;
+  Node *out;
+  long long out_cap;
+  Node *wstack;
+  long long wstack_nodes;
+  SurvRec *surv;
+  long long surv_cap;
+  Ctl *ctl;
+  Ctl *ctl_host;
+  e13_stats stats;
+};
+
+static int cuda_fail(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return 0;
+  fprintf(stderr, "e13: %s: %s\n", what, cudaGetErrorString(e));
+  return 1;
+}
+#define CK(x)                                   \
+  do {                                          \
+    if (cuda_fail((x), #x)) return E13_ERR_CUDA; \
+  } while (0)
+
+static int ensure_consts(e13_ctx *c) {
+  if (c->consts_ready) return E13_OK;
+  uint64_t key[1364], tgt[E13_STAGES + 1];
+  e13_keys(key, tgt);
+  static const long erdos14_stage_step[E13_STAGES + 1] = {0, 2, 22, 90, 268, 944, 3434, 13450, 52068, 208864};
+  static const int exc[E13_STAGES + 1] = {0, 0, 0, 1, 1, 1, 1, 1, 1, 2};
+  u64 t11[E13_STAGES + 2] = {0};
+  int dl[E13_STAGES + 2] = {0};
+  for (int n = 0; n <= E13_STAGES; ++n) {
+    t11[n] = tgt[n];
+    dl[n] = (int)(4 * erdos14_stage_step[n] + 64);
+  }
+  t11[0] = ~0ull;  // never a target
+  CK(cudaMemcpyToSymbol(c_key, key, sizeof key));
+  CK(cudaMemcpyToSymbol(c_tgt, t11, sizeof t11));
+  CK(cudaMemcpyToSymbol(c_deadline, dl, sizeof dl));
+  CK(cudaMemcpyToSymbol(c_exc, exc, sizeof exc));
+  c->consts_ready = true;
+  return E13_OK;
+}
+
+extern "C" int e13_ctx_create(int device, e13_ctx **out) {
+  if (!out) return E13_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return E13_ERR_NO_DEVICE;
+  if (device < 0 || device >= ndev) return E13_ERR_ARG;
+  CK(cudaSetDevice(device));
+  e13_ctx *c = (e13_ctx *)calloc(1, sizeof(e13_ctx));
+  c->device = device;
+  CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&c->ev0));
+  CK(cudaEventCreate(&c->ev1));
+  CK(cudaEventCreate(&c->k0));
+  CK(cudaEventCreate(&c->k1));
+  CK(cudaMallocHost(&c->ctl_host, sizeof(Ctl)));
+  CK(cudaMalloc(&c->ctl, sizeof(Ctl)));
+  *out = c;
+  return E13_OK;
+}
+
+extern "C" void e13_ctx_destroy(e13_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  cudaFree(c->stack);
+  cudaFree(c->out);
+  cudaFree(c->wstack);
+  cudaFree(c->surv);
+  cudaFree(c->ctl);
+  cudaFreeHost(c->ctl_host);
+  cudaEventDestroy(c->ev0);
+  cudaEventDestroy(c->ev1);
+  cudaEventDestroy(c->k0);
+  cudaEventDestroy(c->k1);
+  cudaStreamDestroy(c->stream);
+  free(c);
+}
+
+extern "C" int e13_ctx_device(const e13_ctx *c) { return c ? c->device : 0; }
+
+extern "C" int e13_last_stats(const e13_ctx *c, e13_stats *out) {
+  if (!c || !out) return E13_ERR_ARG;
+  *out = c->stats;
+  return E13_OK;
+}
+
+template <typename T>
+static int grow(T **p, long long *cap, long long want) {
+  if (*cap >= want) return E13_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  CK(cudaMalloc(p, sizeof(T) * (size_t)want));
+  *cap = want;
+  return E13_OK;
+}
+
+static void build_root(const e13_job *job, Node *root) {
+  memset(root, 0, sizeof *root);
+  root->p = kLeft;
+  root->deadline = 4 * 2 + 64;
+  root->nt = 1;
+  root->st0 = -1;
+  root->flags = (signed char)(kFlagAbs | kFlagRel | kFlagKeep);
+  root->pend = -1;
+  root->nintro = (unsigned char)(job->sym_n0 < 0 ? 0 : job->sym_n0);
+  root->budget = (unsigned char)(job->budget < 0 ? 0 : job->budget);
+  for (int i = 0; i < 32; ++i) {
+    unsigned char e = (unsigned char)kEntHalt;
+    if (i < 2 * job->nq) {
+      const int c = job->tab[i];
+      if (c == E13_FREE) e = (unsigned char)kEntFree;
+      else if (c < 0) e = (unsigned char)(kEntUnread | kEntHalt);
+      else e = (unsigned char)(kEntUnread | (unsigned)c);
+    }
+    root->ent[i] = e;
+  }
+}
+
+static void decode_survivor(const SurvRec &r, int nq, e13_survivor *s) {
+  memset(s, 0, sizeof *s);
+  for (int i = 0; i < E13_MAXCELLS; ++i) s->tab[i] = E13_HALT;
+  uint32_t mask = 0;
+  for (int i = 0; i < 2 * nq; ++i) {
+    const unsigned e = r.ent[i];
+    if (e == kEntFree) {
+      s->tab[i] = E13_FREE;
+    } else {
+      if (!(e & kEntUnread)) mask |= 1u << i;
+      const unsigned v = e & 0x7Fu;
+      s->tab[i] = (v & kEntHalt) ? E13_HALT : (int)v;
+    }
+  }
+  s->read_mask = mask;
+  s->st0 = r.st0;
+  s->head0 = r.head0;
+  s->abs_ok = r.abs_ok;
+  s->rel_ok = r.rel_ok;
+  s->steps = r.t;
+}
+
+extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuning, e13_counts *counts,
+                          e13_survivor *surv, int surv_cap, int *nsurv) {
+  if (!c || !job || !counts || !nsurv || (surv_cap > 0 && !surv) || surv_cap < 0) return E13_ERR_ARG;
+  if (job->nq < 1 || job->nq > 16) return E13_ERR_NQ;
+  if (job->budget < 0) return E13_ERR_FMAX;
+  e13_tuning tu;
+  e13_default_tuning(&tu);
+  if (tuning) {
+    if (tuning->kernel == E13_KERNEL_PLAIN || tuning->kernel == E13_KERNEL_PERSISTENT) tu.kernel = tuning->kernel;
+    if (tuning->block) tu.block = tuning->block;
+    if (tuning->slice) tu.slice = tuning->slice;
+    if (tuning->warp_stack) tu.warp_stack = tuning->warp_stack;
+    if (tuning->step_cap) tu.step_cap = tuning->step_cap;
+    if (tuning->batch) tu.batch = tuning->batch;
+    if (tuning->epoch_us) tu.epoch_us = tuning->epoch_us;
+    if (tuning->epochs_per_graph) tu.epochs_per_graph = tuning->epochs_per_graph;
+    if (tuning->starve_pct) tu.starve_pct = tuning->starve_pct;
+    tu.run_skip = tuning->run_skip;
+    if (tuning->stack_nodes) tu.stack_nodes = tuning->stack_nodes;
+  }
+  if (tu.block < 64 || tu.block > 768 || tu.block % 32) return E13_ERR_ARG;
+  if (tu.slice < 1 || tu.warp_stack < 1 || tu.warp_stack > 4096) return E13_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  int rc = ensure_consts(c);
+  if (rc) return rc;
+  memset(&c->stats, 0, sizeof c->stats);
+
+  const bool persist = tu.kernel == E13_KERNEL_PERSISTENT;
+  const int blocks = c->nsm;
+  const long long nwarps = (long long)blocks * tu.block / 32;
+  const long long stack_nodes = tu.stack_nodes > 0 ? tu.stack_nodes : (4LL << 20);
+  const long long dump_room = nwarps * (32 + (persist ? tu.warp_stack : 0));
+  long long out_nodes, batch_max;
+  if (persist) {
+    batch_max = tu.batch > 0 ? tu.batch : nwarps * 16;
+    out_nodes = 2 * dump_room + 65536;
+  } else {
+    batch_max = tu.batch > 0 ? tu.batch : 16384;
+    out_nodes = batch_max * (4LL * job->nq + 1) + nwarps * 32 + 1024;
+  }
+  if ((rc = grow(&c->stack, &c->stack_cap, stack_nodes))) return rc;
+  if ((rc = grow(&c->out, &c->out_cap, out_nodes))) return rc;
+  if (persist && (rc = grow(&c->wstack, &c->wstack_nodes, nwarps * tu.warp_stack))) return rc;
+  const long long scap = std::max<long long>(surv_cap, 1024);
+  if ((rc = grow(&c->surv, &c->surv_cap, scap))) return rc;
+
+  Params P;
+  P.nq = job->nq;
+  P.nv = 4 * job->nq;
+  P.sym_lo = job->sym_lo;
+  P.sym_hi = job->sym_hi;
+  P.slice = tu.slice;
+  P.step_cap = tu.step_cap;
+  P.wdepth = tu.warp_stack;
+  P.starve_limit = (int)std::max<long long>(1, nwarps * tu.starve_pct / 100);
+  P.out_cap = c->out_cap;
+  P.out_soft = c->out_cap - dump_room - 1024;
+  P.surv_cap = c->surv_cap;
+  P.epoch_ns = (long long)tu.epoch_us * 1000LL;
+  P.stack = c->stack;
+  P.out = c->out;
+  P.wstack = c->wstack;
+  P.surv = c->surv;
+  P.ctl = c->ctl;
+
+  const size_t smem = kKeySmemBytes + (size_t)(kTapeWords + 16) * tu.block * 4;
+  if (persist) CK(cudaFuncSetAttribute(search_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  else CK(cudaFuncSetAttribute(search_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+
+  // the root: blank tape, every cell unread
+  Node root;
+  build_root(job, &root);
+  memset(c->ctl_host, 0, sizeof(Ctl));
+  c->ctl_host->top = 1;
+  c->ctl_host->batch = 1;
+  c->ctl_host->peak = 1;
+  CK(cudaMemcpyAsync(c->stack, &root, sizeof root, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaEventRecord(c->ev0, c->stream));
+
+  const int move_blocks = c->nsm * 4;
+  long long launches = 0, search_launches = 0;
+  int err = 0;
+  if (persist) {
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    for (int e = 0; e < tu.epochs_per_graph; ++e) {
+      search_kernel<true><<<blocks, tu.block, smem, c->stream>>>(P);
+      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out);
+      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, batch_max);
+    }
+    CK(cudaStreamEndCapture(c->stream, &graph));
+    CK(cudaGraphInstantiate(&exec, graph, 0));
+    for (;;) {
+      CK(cudaGraphLaunch(exec, c->stream));
+      launches += 3LL * tu.epochs_per_graph;
+      search_launches += tu.epochs_per_graph;
+      CK(cudaMemcpyAsync(c->ctl_host, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (c->ctl_host->error) {
+        err = (c->ctl_host->error & kErrOutFull) ? E13_ERR_OVERFLOW : E13_ERR_OVERFLOW;
+        break;
+      }
+      if (c->ctl_host->top > c->stack_cap - (long long)out_nodes) {
+        err = E13_ERR_OVERFLOW;
+        break;
+      }
+      if (c->ctl_host->top == 0) break;
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+  } else {
+    for (;;) {
+      search_kernel<false><<<blocks, tu.block, smem, c->stream>>>(P);
+      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out);
+      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, batch_max);
+      launches += 3;
+      search_launches += 1;
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(c->ctl_host, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (c->ctl_host->error) {
+        err = E13_ERR_OVERFLOW;
+        break;
+      }
+      if (c->ctl_host->top > c->stack_cap - (long long)out_nodes) {
+        err = E13_ERR_OVERFLOW;
+        break;
+      }
+      if (c->ctl_host->top == 0) break;
+    }
+  }
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  CK(cudaGetLastError());
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  c->stats.device_ms = ms;
+  c->stats.launches = launches;
+  c->stats.search_kernel_launches = search_launches;
+  c->stats.epochs = c->ctl_host->launches;
+  c->stats.peak_nodes = c->ctl_host->peak;
+  if (err) return err;
+
+  const Ctl &h = *c->ctl_host;
+  memset(counts, 0, sizeof *counts);
+  counts->leaves = h.leaves;
+  counts->steps = h.steps;
+  counts->survivors = h.nsurv;
+  for (int j = 0; j <= E13_STAGES; ++j) counts->hist[j] = h.hist[j];
+  const long long ns = (long long)h.nsurv;
+  *nsurv = (int)std::min<long long>(ns, 0x7FFFFFFF);
+  const long long ncopy = std::min<long long>(ns, std::min<long long>(surv_cap, c->surv_cap));
+  if (ncopy > 0) {
+    std::vector<SurvRec> recs((size_t)ncopy);
+    CK(cudaMemcpy(recs.data(), c->surv, sizeof(SurvRec) * (size_t)ncopy, cudaMemcpyDeviceToHost));
+    for (long long i = 0; i < ncopy; ++i) decode_survivor(recs[(size_t)i], job->nq, &surv[i]);
+  }
+  if (ns > surv_cap || ns > c->surv_cap) return E13_ERR_SURV_CAP;
+  return E13_OK;
+}
+
+extern "C" int e13_run_full(e13_ctx *c, const int32_t *tabs, int n, int nq, int64_t *out) {
+  if (!c || !tabs || !out || n < 0 || nq < 1 || nq > 16) return E13_ERR_ARG;
+  if (n == 0) return E13_OK;
+  CK(cudaSetDevice(c->device));
+  int rc = ensure_consts(c);
+  if (rc) return rc;
+  int *d_tabs = nullptr;
+  long long *d_out = nullptr;
+  CK(cudaMalloc(&d_tabs, sizeof(int) * E13_MAXCELLS * (size_t)n));
+  CK(cudaMalloc(&d_out, sizeof(long long) * 7 * (size_t)n));
+  CK(cudaMemcpyAsync(d_tabs, tabs, sizeof(int) * E13_MAXCELLS * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+  const int bd = 256;
+  const size_t smem = kKeySmemBytes + (size_t)(kTapeWords + 16) * bd * 4;
+  CK(cudaFuncSetAttribute(run_full_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  run_full_kernel<<<(n + bd - 1) / bd, bd, smem, c->stream>>>(d_tabs, n, nq, d_out);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, d_out, sizeof(long long) * 7 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(d_tabs);
+  cudaFree(d_out);
+  return E13_OK;
+}

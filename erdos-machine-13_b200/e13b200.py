@@ -1,0 +1,272 @@
+"""Python access to libe13b200.so through its C-ABI (include/e13.h).
+
+This module only marshals arguments; all search work runs in the CUDA kernels
+of the shared library.  There is no CPU fallback: without the built library or
+without a CUDA device the calls raise.
+
+The function names follow the reference's program structure
+(src/e13search.c: load, setup, run_delete, run_full, report; src/recheck.c).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libe13b200.so")
+
+E13_MAXCELLS = 32
+E13_HALT = -1
+E13_FREE = -2
+KERNEL_PLAIN = 0
+KERNEL_PERSISTENT = 1
+
+ERRORS = {
+    -1: "bad argument", -2: "forced cells exceed FMAX", -3: "symmetric state named by a fixed cell or has one",
+    -4: "start state in the symmetric states", -5: "CUDA error", -6: "frontier stack overflow",
+    -7: "survivor buffer too small", -8: "too many states", -9: "cannot open machine file",
+    -10: "device wait timed out", -11: "no CUDA device",
+}
+
+
+class E13Error(RuntimeError):
+    def __init__(self, code, what=""):
+        super().__init__(f"{what}: {ERRORS.get(code, code)} ({code})")
+        self.code = code
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("X", ctypes.c_int32), ("nq", ctypes.c_int32), ("tab", ctypes.c_int32 * E13_MAXCELLS),
+                ("budget", ctypes.c_int32), ("nforced", ctypes.c_int32), ("sym_lo", ctypes.c_int32),
+                ("sym_hi", ctypes.c_int32), ("sym_n0", ctypes.c_int32)]
+
+
+class Counts(ctypes.Structure):
+    _fields_ = [("leaves", ctypes.c_uint64), ("survivors", ctypes.c_uint64), ("steps", ctypes.c_uint64),
+                ("hist", ctypes.c_uint64 * 10)]
+
+    def as_dict(self):
+        return dict(leaves=self.leaves, survivors=self.survivors, steps=self.steps, hist=list(self.hist))
+
+
+class Survivor(ctypes.Structure):
+    _fields_ = [("tab", ctypes.c_int32 * E13_MAXCELLS), ("read_mask", ctypes.c_uint32), ("st0", ctypes.c_int32),
+                ("head0", ctypes.c_int32), ("abs_ok", ctypes.c_int32), ("rel_ok", ctypes.c_int32),
+                ("steps", ctypes.c_int64)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("kernel", ctypes.c_int32), ("block", ctypes.c_int32), ("slice", ctypes.c_int32),
+                ("warp_stack", ctypes.c_int32), ("step_cap", ctypes.c_int32), ("batch", ctypes.c_int32),
+                ("epoch_us", ctypes.c_int32), ("epochs_per_graph", ctypes.c_int32), ("starve_pct", ctypes.c_int32),
+                ("run_skip", ctypes.c_int32), ("stack_nodes", ctypes.c_int64)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("device_ms", ctypes.c_double), ("launches", ctypes.c_int64), ("epochs", ctypes.c_int64),
+                ("peak_nodes", ctypes.c_int64), ("search_kernel_launches", ctypes.c_int64),
+                ("search_kernel_ms", ctypes.c_double)]
+
+
+E13_CHECK_MAX_NMAX = 20
+E13_CHECK_MAX_ONES = 64
+
+
+class CheckIn(ctypes.Structure):
+    _fields_ = [("nq", ctypes.c_int32), ("st0", ctypes.c_int32), ("rel", ctypes.c_int32), ("head0", ctypes.c_int64),
+                ("kind", ctypes.c_int8 * E13_MAXCELLS), ("write", ctypes.c_int8 * E13_MAXCELLS),
+                ("move", ctypes.c_int8 * E13_MAXCELLS), ("next", ctypes.c_int8 * E13_MAXCELLS)]
+
+
+class CheckOut(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("fail_stage", ctypes.c_int32), ("free_state", ctypes.c_int32),
+                ("free_sym", ctypes.c_int32), ("fail_t", ctypes.c_int64), ("fail_head", ctypes.c_int64),
+                ("stages_done", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("stage_t", ctypes.c_int64 * (E13_CHECK_MAX_NMAX + 1)),
+                ("minhead", ctypes.c_int64 * (E13_CHECK_MAX_NMAX + 1)),
+                ("nones", ctypes.c_int32 * (E13_CHECK_MAX_NMAX + 1)),
+                ("leftmost", ctypes.c_int64 * (E13_CHECK_MAX_NMAX + 1)),
+                ("ones_cells", (ctypes.c_int32 * E13_CHECK_MAX_ONES) * (E13_CHECK_MAX_NMAX + 1))]
+
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    """Loads libe13b200.so (building it first if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER
+        I = ctypes.c_int
+        L.e13_keys.argtypes = [P(ctypes.c_uint64), P(ctypes.c_uint64)]
+        L.e13_keys.restype = None
+        L.e13_parse_cell.argtypes = [ctypes.c_char_p]
+        L.e13_load_machine.argtypes = [ctypes.c_char_p, P(ctypes.c_int32)]
+        L.e13_parse_machine.argtypes = [ctypes.c_char_p, P(ctypes.c_int32)]
+        L.e13_setup.argtypes = [P(ctypes.c_int32), I, I, I, ctypes.c_char_p, I, I, P(Job)]
+        L.e13_format_survivor.argtypes = [P(Job), P(Survivor), ctypes.c_char_p, ctypes.c_size_t]
+        L.e13_format_summary.argtypes = [P(Job), P(Counts), ctypes.c_double, ctypes.c_char_p, ctypes.c_size_t]
+        L.e13_default_tuning.argtypes = [P(Tuning)]
+        L.e13_default_tuning.restype = None
+        L.e13_ctx_create.argtypes = [I, P(ctypes.c_void_p)]
+        L.e13_ctx_destroy.argtypes = [ctypes.c_void_p]
+        L.e13_ctx_destroy.restype = None
+        L.e13_search.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Counts), P(Survivor), I, P(I)]
+        L.e13_last_stats.argtypes = [ctypes.c_void_p, P(Stats)]
+        L.e13_run_full.argtypes = [ctypes.c_void_p, P(ctypes.c_int32), I, I, P(ctypes.c_int64)]
+        L.e13_check.argtypes = [ctypes.c_void_p, P(CheckIn), I, I, I, P(CheckOut)]
+        L.e13_parse_survivor_line.argtypes = [ctypes.c_char_p, P(CheckIn)]
+        L.e13_format_recheck.argtypes = [P(CheckOut), I, ctypes.c_char_p, ctypes.c_size_t]
+        L.e13_format_deep.argtypes = [P(CheckIn), P(CheckOut), I, ctypes.c_char_p, ctypes.c_size_t]
+        _lib = L
+    return _lib
+
+
+EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine", "e13_setup",
+            "e13_format_survivor", "e13_format_summary", "e13_default_tuning", "e13_ctx_create", "e13_ctx_destroy",
+            "e13_search", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
+            "e13_format_recheck", "e13_format_deep"]
+
+
+def keys():
+    k = (ctypes.c_uint64 * 1364)()
+    t = (ctypes.c_uint64 * 10)()
+    lib().e13_keys(k, t)
+    return list(k), list(t)
+
+
+def load_machine(path: str) -> list[int]:
+    base = (ctypes.c_int32 * E13_MAXCELLS)()
+    nq = lib().e13_load_machine(path.encode(), base)
+    if nq < 0:
+        raise E13Error(nq, path)
+    return list(base)[: 2 * nq]
+
+
+def parse_machine(text: str) -> list[int]:
+    base = (ctypes.c_int32 * E13_MAXCELLS)()
+    nq = lib().e13_parse_machine(text.encode(), base)
+    return list(base)[: 2 * nq]
+
+
+def cell_index(name: str) -> int:
+    return 2 * (ord(name[0]) - ord("A")) + int(name[1])
+
+
+def setup(base, X, fmax=0, free_cells=None, lo=-1, hi=-1):
+    """Returns (status, Job); status 0 or a negative e13 error (the job is
+    still filled as far as the reference's setup() gets)."""
+    b = (ctypes.c_int32 * E13_MAXCELLS)(*(list(base) + [E13_HALT] * (E13_MAXCELLS - len(base))))
+    fb = None
+    if free_cells is not None:
+        arr = bytearray(E13_MAXCELLS)
+        for c in free_cells:
+            arr[cell_index(c) if isinstance(c, str) else c] = 1
+        fb = bytes(arr)
+    job = Job()
+    r = lib().e13_setup(b, len(base) // 2, X, fmax, fb, lo, hi, ctypes.byref(job))
+    return r, job
+
+
+def tuning(**kw) -> Tuning:
+    t = Tuning()
+    lib().e13_default_tuning(ctypes.byref(t))
+    for k, v in kw.items():
+        setattr(t, k, v)
+    return t
+
+
+class Context:
+    """A device context (one CUDA device, one stream, reusable buffers)."""
+
+    def __init__(self, device: int = 0):
+        self.h = ctypes.c_void_p()
+        r = lib().e13_ctx_create(device, ctypes.byref(self.h))
+        if r:
+            raise E13Error(r, "e13_ctx_create")
+
+    def close(self):
+        if self.h:
+            lib().e13_ctx_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def search(self, job: Job, tune: Tuning | None = None, surv_cap: int = 1 << 16):
+        counts = Counts()
+        surv = (Survivor * max(surv_cap, 1))()
+        ns = ctypes.c_int()
+        r = lib().e13_search(self.h, ctypes.byref(job), ctypes.byref(tune) if tune else None, ctypes.byref(counts),
+                             surv, surv_cap, ctypes.byref(ns))
+        if r and r != -7:
+            raise E13Error(r, "e13_search")
+        return counts, [surv[i] for i in range(min(ns.value, surv_cap))]
+
+    def stats(self) -> Stats:
+        s = Stats()
+        lib().e13_last_stats(self.h, ctypes.byref(s))
+        return s
+
+    def run_full(self, tabs, nq):
+        n = len(tabs)
+        arr = (ctypes.c_int32 * (E13_MAXCELLS * max(n, 1)))()
+        for i, t in enumerate(tabs):
+            for j, v in enumerate(t):
+                arr[E13_MAXCELLS * i + j] = v
+        out = (ctypes.c_int64 * (7 * max(n, 1)))()
+        r = lib().e13_run_full(self.h, arr, n, nq, out)
+        if r:
+            raise E13Error(r, "e13_run_full")
+        return [list(out[7 * i: 7 * i + 7]) for i in range(n)]
+
+    def check(self, ins, nmax, mode=0):
+        n = len(ins)
+        arr = (CheckIn * max(n, 1))(*ins)
+        out = (CheckOut * max(n, 1))()
+        r = lib().e13_check(self.h, arr, n, nmax, mode, out)
+        if r:
+            raise E13Error(r, "e13_check")
+        return [out[i] for i in range(n)]
+
+
+def survivor_line(job: Job, s: Survivor) -> str:
+    buf = ctypes.create_string_buffer(1024)
+    n = lib().e13_format_survivor(ctypes.byref(job), ctypes.byref(s), buf, 1024)
+    if n < 0:
+        raise E13Error(n, "e13_format_survivor")
+    return buf.value.decode()
+
+
+def summary_line(job: Job, c: Counts, wall: float) -> str:
+    buf = ctypes.create_string_buffer(512)
+    lib().e13_format_summary(ctypes.byref(job), ctypes.byref(c), wall, buf, 512)
+    return buf.value.decode()
+
+
+def parse_survivor_line(line: str) -> CheckIn | None:
+    ci = CheckIn()
+    return ci if lib().e13_parse_survivor_line(line.encode(), ctypes.byref(ci)) else None
+
+
+def format_recheck(o: CheckOut, nmax: int) -> str:
+    buf = ctypes.create_string_buffer(8192)
+    lib().e13_format_recheck(ctypes.byref(o), nmax, buf, 8192)
+    return buf.value.decode()
+
+
+def format_deep(ci: CheckIn, o: CheckOut, nmax: int) -> str:
+    buf = ctypes.create_string_buffer(8192)
+    lib().e13_format_deep(ctypes.byref(ci), ctypes.byref(o), nmax, buf, 8192)
+    return buf.value.decode()

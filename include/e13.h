@@ -1,0 +1,230 @@
+/*
+ * e13.h -- C-ABI of libe13b200.so, the B200 (sm_100a) tree-normal-form search
+ * over 2-symbol Turing machines near erdos_14.
+ *
+ * Plain C types only: pointers, sizes and int status codes.  The caller owns
+ * every host buffer; a context owns the device memory it allocates.  One host
+ * thread per context.  Functions return E13_OK (0) or a negative E13_ERR_*.
+ *
+ * The reference has no plugin or FFI; its boundary is the e13search process
+ * (src/e13search.c:435-513) and the recheck/deep programs.  Each entry point
+ * below names the reference code whose behaviour it takes over.
+ */
+#ifndef E13_H
+#define E13_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define E13_MAXQ 16          /* rows a machine file may hold (src/e13search.c:63) */
+#define E13_MAXCELLS 32
+#define E13_STAGES 9         /* stage starts n = 1..9 (src/e13search.c:58) */
+#define E13_TAPE_LEFT 64     /* window: cells -64..1299 (src/e13search.c:59-61) */
+#define E13_TAPE_RIGHT 1300
+
+/* cell codes, as in the reference: (next << 2) | (dir << 1) | write, dir 1 = R */
+#define E13_HALT (-1)
+#define E13_FREE (-2)        /* FORCED in src/e13search.c:66: any move at first read */
+
+enum {
+  E13_OK = 0,
+  E13_ERR_ARG = -1,          /* bad argument (null pointer, size out of range) */
+  E13_ERR_FMAX = -2,         /* forced cells exceed FMAX: the reference skips X (src/e13search.c:353) */
+  E13_ERR_SYM_NAMED = -3,    /* symmetric state named by / owning a fixed cell (src/e13search.c:344-348) */
+  E13_ERR_SYM_START = -4,    /* start state among the symmetric states (src/e13search.c:349) */
+  E13_ERR_CUDA = -5,         /* a CUDA call failed (device, memory, launch) */
+  E13_ERR_OVERFLOW = -6,     /* frontier stack capacity exceeded */
+  E13_ERR_SURV_CAP = -7,     /* more survivors than the caller's buffer holds (counts stay exact) */
+  E13_ERR_NQ = -8,           /* more states than the device path supports (nq <= 16) */
+  E13_ERR_IO = -9,           /* machine file missing or unreadable (src/e13search.c:113) */
+  E13_ERR_TIMEOUT = -10,     /* a device wait ran out (bounded waits; no hang) */
+  E13_ERR_NO_DEVICE = -11    /* no CUDA device: there is no CPU fallback */
+};
+
+/* A prepared candidate family: base machine with state X deleted.
+   Built by e13_setup (src/e13search.c:317-355 setup, :423-426 set_sym). */
+typedef struct e13_job {
+  int32_t X;                 /* deleted base state, -1 = none */
+  int32_t nq;                /* states after the deletion */
+  int32_t tab[E13_MAXCELLS]; /* codes, renumbered; E13_FREE for free cells */
+  int32_t budget;            /* further changes allowed (delete mode); 0 in free mode */
+  int32_t nforced;           /* rules into X (nF) */
+  int32_t sym_lo, sym_hi;    /* interchangeable states, renumbered; -1 = off */
+  int32_t sym_n0;            /* leading symmetric states already named by fixed cells */
+} e13_job;
+
+/* Totals of one search (src/e13search.c:413-416 summary line). */
+typedef struct e13_counts {
+  uint64_t leaves;
+  uint64_t survivors;
+  uint64_t steps;
+  uint64_t hist[E13_STAGES + 1]; /* dead leaves by last stage reached */
+} e13_counts;
+
+/* One survivor (src/e13search.c:184-200 report): the table as the search
+   left it, with a read mask (bit i: cell i was read, i.e. fixed). */
+typedef struct e13_survivor {
+  int32_t tab[E13_MAXCELLS]; /* codes; E13_FREE / E13_HALT print as --- */
+  uint32_t read_mask;
+  int32_t st0, head0, abs_ok, rel_ok;
+  int64_t steps;             /* step of the stage-9 start */
+} e13_survivor;
+
+/* Search kernels. */
+enum {
+  E13_KERNEL_PLAIN = 0,      /* one launch per frontier batch, host sync per launch */
+  E13_KERNEL_PERSISTENT = 1  /* per-warp DFS epochs from a device work queue, graph-captured */
+};
+
+/* Tunables of the device search (0 = library default; see e13_default_tuning). */
+typedef struct e13_tuning {
+  int32_t kernel;            /* E13_KERNEL_* */
+  int32_t block;             /* lanes (threads) per CTA: 128..896, multiple of 32 */
+  int32_t slice;             /* steps per round between warp-level refills */
+  int32_t warp_stack;        /* nodes in each warp's private DFS stack (persistent) */
+  int32_t step_cap;          /* plain kernel: steps per work item before it is requeued */
+  int32_t batch;             /* nodes taken from the frontier per launch / epoch (0 = auto) */
+  int32_t epoch_us;          /* persistent: wall-clock bound of one epoch, microseconds */
+  int32_t epochs_per_graph;  /* persistent: epochs captured in one CUDA graph */
+  int32_t starve_pct;        /* persistent: end an epoch when this % of warps starve */
+  int32_t run_skip;          /* 1: advance whole words across runs of a self-loop (exact) */
+  int64_t stack_nodes;       /* frontier stack capacity in nodes (0 = auto) */
+} e13_tuning;
+
+/* Runtime statistics of the last search on a context. */
+typedef struct e13_stats {
+  double device_ms;          /* CUDA-event time of the search on its stream */
+  int64_t launches;          /* kernel launches (all kinds) */
+  int64_t epochs;            /* persistent epochs / plain frontier launches */
+  int64_t peak_nodes;        /* peak frontier stack */
+  int64_t search_kernel_launches;
+  double search_kernel_ms;   /* CUDA-event time summed over the search kernel's launches */
+} e13_stats;
+
+typedef struct e13_ctx e13_ctx;
+
+/* ---- host-side helpers (no device needed) ---- */
+
+/* Zobrist keys of the 1364 window cells and stage-start block hashes TGT[0..9]
+   (src/e13search.c:98-103, :437-444). */
+void e13_keys(uint64_t key[1364], uint64_t tgt[E13_STAGES + 1]);
+
+/* One cell "<w><L|R><next>" or "---" (src/e13search.c:105-108). */
+int e13_parse_cell(const char *s);
+
+/* Machine file: up to 16 rows of two cells (src/e13search.c:110-121).
+   Returns the number of states, or E13_ERR_IO. */
+int e13_load_machine(const char *path, int32_t base[E13_MAXCELLS]);
+/* Same from text in memory. */
+int e13_parse_machine(const char *text, int32_t base[E13_MAXCELLS]);
+
+/* Candidate construction (src/e13search.c:317-355 setup, :423-426 set_sym).
+   free_cells: 2*nq0 flags in base numbering (NULL = delete mode with fmax).
+   lo < 0: no symmetry.  Returns E13_OK, E13_ERR_FMAX, E13_ERR_SYM_NAMED or
+   E13_ERR_SYM_START; job is filled as far as the reference gets. */
+int e13_setup(const int32_t *base, int nq0, int X, int fmax, const uint8_t *free_cells, int lo, int hi,
+              e13_job *job);
+
+/* Survivor line in the reference's format (src/e13search.c:184-200), no
+   newline.  Returns the length written (< len) or E13_ERR_ARG. */
+int e13_format_survivor(const e13_job *job, const e13_survivor *s, char *buf, size_t len);
+
+/* Summary line (src/e13search.c:413-416) without "split=/front=" (device path)
+   and with wall seconds as given.  Returns the length written. */
+int e13_format_summary(const e13_job *job, const e13_counts *c, double wall_s, char *buf, size_t len);
+
+/* Fills t with the library defaults for this device. */
+void e13_default_tuning(e13_tuning *t);
+
+/* ---- device path ---- */
+
+/* Creates a context on CUDA device `device` (allocations happen lazily on
+   the first search and are kept for reuse).  Returns E13_OK or an error. */
+int e13_ctx_create(int device, e13_ctx **out);
+void e13_ctx_destroy(e13_ctx *ctx);
+
+/* The search for one job (src/e13search.c:357-420 run_delete; GPU reference
+   src/e13gpu.py:381-461): enumerates every TNF leaf on the device.
+   counts: exact totals.  surv: up to surv_cap records; *nsurv = survivors
+   found (may exceed surv_cap: E13_ERR_SURV_CAP, counts still exact).
+   tuning may be NULL (defaults).  Output order of survivors is undefined, as
+   in the reference (src/e13search.c:185): compare sorted lines. */
+int e13_search(e13_ctx *ctx, const e13_job *job, const e13_tuning *tuning, e13_counts *counts,
+               e13_survivor *surv, int surv_cap, int *nsurv);
+
+/* Statistics of the last e13_search on this context. */
+int e13_last_stats(const e13_ctx *ctx, e13_stats *out);
+
+/* Whole-table runs from the blank tape on the device, one machine per lane
+   (src/e13search.c:428-433 run_full; modes base/mutant :447-460).
+   tabs: n tables of 2*nq codes (stride E13_MAXCELLS); out: per machine
+   {survived, stage, st0, head0, abs, rel, steps} as 7 int64. */
+int e13_run_full(e13_ctx *ctx, const int32_t *tabs, int n, int nq, int64_t *out);
+
+/* ---- hash-free deep checker (src/recheck.c, src/deep.c) ---- */
+
+enum { E13_CHECK_RECHECK = 0, E13_CHECK_DEEP = 1 };
+
+/* Input: one survivor as the checkers parse it (src/recheck.c:31-56). */
+typedef struct e13_check_in {
+  int32_t nq;
+  int32_t st0;
+  int32_t rel;               /* 1: head rule relative to the block end (!abs && rel) */
+  int64_t head0;
+  int8_t kind[E13_MAXCELLS]; /* 0 move, 1 halt, 2 free cell never read */
+  int8_t write[E13_MAXCELLS];
+  int8_t move[E13_MAXCELLS]; /* +1 R, -1 L */
+  int8_t next[E13_MAXCELLS];
+} e13_check_in;
+
+/* Outcome per machine. */
+enum {
+  E13_CHK_OK = 0,            /* every stage 1..nmax reached */
+  E13_CHK_LIMIT = 1,         /* stage not reached within the step limit */
+  E13_CHK_OFFTAPE = 2,
+  E13_CHK_FREE_READ = 3,     /* a never-read free cell was read */
+  E13_CHK_HALT = 4
+};
+
+#define E13_CHECK_MAX_NMAX 20
+#define E13_CHECK_MAX_ONES 64  /* counter ones recorded per stage start */
+
+typedef struct e13_check_out {
+  int32_t status;            /* E13_CHK_* */
+  int32_t fail_stage;        /* stage at which it failed (status != OK) */
+  int32_t free_state, free_sym; /* for E13_CHK_FREE_READ */
+  int64_t fail_t;            /* step at the failure */
+  int64_t fail_head;         /* head at the failure (deep's off-tape print) */
+  int32_t stages_done;       /* stage starts found */
+  int32_t pad;
+  int64_t stage_t[E13_CHECK_MAX_NMAX + 1];   /* step of each stage start */
+  int64_t minhead[E13_CHECK_MAX_NMAX + 1];   /* leftmost head before each start */
+  int32_t nones[E13_CHECK_MAX_NMAX + 1];     /* ones at cells <= -3 (all of them) */
+  int64_t leftmost[E13_CHECK_MAX_NMAX + 1];  /* leftmost one at cells <= -3 (0: none) */
+  int32_t ones_cells[E13_CHECK_MAX_NMAX + 1][E13_CHECK_MAX_ONES]; /* their cells, -3 downwards */
+} e13_check_out;
+
+/* Re-runs machines from the blank tape to stage nmax without hashing, with
+   recheck.c's step limit and tape (mode E13_CHECK_RECHECK, src/recheck.c:57-92)
+   or deep.c's (E13_CHECK_DEEP, src/deep.c:49-80). */
+int e13_check(e13_ctx *ctx, const e13_check_in *in, int n, int nmax, int mode, e13_check_out *out);
+
+/* Parses a SURVIVOR line into a checker input (src/recheck.c:28-56).
+   Returns 1 on success, 0 if the line has no table. */
+int e13_parse_survivor_line(const char *line, e13_check_in *in);
+
+/* recheck.c's verdict text for one machine (src/recheck.c:71-99) from the
+   device result; returns 1 if CONSISTENT. */
+int e13_format_recheck(const e13_check_out *o, int nmax, char *buf, size_t len);
+
+/* deep.c's per-machine text after "survivor <id> " (src/deep.c:53-81). */
+int e13_format_deep(const e13_check_in *in, const e13_check_out *o, int nmax, char *buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* E13_H */

@@ -1,0 +1,143 @@
+"""Parity of the CUDA search (both kernels, through the C-ABI) with the
+reference: golden counts and survivor sets from the reference's result logs,
+and seeded random searches against the CPU oracle."""
+import random
+
+import pytest
+
+import e13b200 as E
+import oracle_lib as O
+from gpu_common import check_entry, ctx, golden_lines, run_entry
+
+pytestmark = pytest.mark.gpu
+
+KERNELS = {"plain": E.KERNEL_PLAIN, "persistent": E.KERNEL_PERSISTENT}
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
+@pytest.mark.parametrize("name", ["local_edits_f2", "doubling_X0", "doubling_X2", "split_test", "split_test_free",
+                                  "counters_f2_base_01", "counters_f2_base_44"])
+def test_small_golden(searches, name, kernel):
+    e = searches[name]
+    per_x, lines = run_entry(e, E.tuning(kernel=KERNELS[kernel]))
+    check_entry(e, per_x)
+    if "survivors_file" in e:
+        assert lines == golden_lines(e)
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_local_edits_f3(searches, kernel):
+    e = searches["local_edits_f3"]
+    per_x, lines = run_entry(e, E.tuning(kernel=KERNELS[kernel]))
+    check_entry(e, per_x)
+    assert lines == golden_lines(e)
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_division_v4(searches, kernel):
+    e = searches["division_v4"]
+    per_x, lines = run_entry(e, E.tuning(kernel=KERNELS[kernel]))
+    check_entry(e, per_x)
+    assert lines == []
+
+
+def test_counter_sym(searches):
+    e = searches["counter_sym"]
+    per_x, lines = run_entry(e, E.tuning(kernel=E.KERNEL_PERSISTENT))
+    check_entry(e, per_x)
+    assert lines == golden_lines(e)
+
+
+def test_local_edits_f4(searches):
+    """configs[1] at FMAX = 4: 5,986,617,022 leaves, 57 survivors."""
+    e = searches["local_edits_f4"]
+    per_x, lines = run_entry(e, E.tuning(kernel=E.KERNEL_PERSISTENT))
+    check_entry(e, per_x)
+    assert lines == golden_lines(e)
+
+
+def _random_cases(n, seed):
+    rng = random.Random(seed)
+    base = O.load_machine("erdos_14.txt")
+    cells = [f"{chr(65 + q)}{a}" for q in range(14) for a in (0, 1)]
+    out = []
+    while len(out) < n:
+        X = rng.randrange(14)
+        if rng.random() < 0.5:
+            free = rng.sample([c for c in cells if ord(c[0]) - 65 != X], rng.randint(2, 4))
+            r, job = O.setup(base, X, free_cells=free)
+            if r >= 0:
+                out.append(("free", X, free, None))
+        else:
+            fmax = rng.randint(1, 2)
+            r, job = O.setup(base, X, fmax=fmax)
+            if r >= 0:
+                out.append(("delete", X, None, fmax))
+    return out
+
+
+@pytest.mark.parametrize("case", _random_cases(8, 13))
+def test_random_searches_vs_oracle(case):
+    mode, X, free, fmax = case
+    base = O.load_machine("erdos_14.txt")
+    if mode == "free":
+        r, jo = O.setup(base, X, free_cells=free)
+        _, job = E.setup(base, X, free_cells=free)
+    else:
+        r, jo = O.setup(base, X, fmax=fmax)
+        _, job = E.setup(base, X, fmax=fmax)
+    exp, recs = O.search(jo)
+    exp_lines = sorted(O.survivor_line(X, rr, jo.nq) for rr in recs)
+    for k in (E.KERNEL_PLAIN, E.KERNEL_PERSISTENT):
+        c, surv = ctx().search(job, E.tuning(kernel=k))
+        assert c.as_dict() == exp
+        assert sorted(E.survivor_line(job, s) for s in surv) == exp_lines
+
+
+def test_symmetric_vs_oracle():
+    base = O.load_machine("erdos_14.txt")
+    free = ["H0", "H1", "I0", "I1"]
+    r, jo = O.setup(base, 9, free_cells=free, lo=3, hi=9)
+    _, job = E.setup(base, 9, free_cells=free, lo=3, hi=9)
+    exp, recs = O.search(jo)
+    for k in (E.KERNEL_PLAIN, E.KERNEL_PERSISTENT):
+        c, surv = ctx().search(job, E.tuning(kernel=k))
+        assert c.as_dict() == exp
+
+
+@pytest.mark.parametrize("tune", [dict(slice=1), dict(slice=7, warp_stack=1), dict(block=256, slice=64),
+                                  dict(warp_stack=3, starve_pct=1, epoch_us=200),
+                                  dict(kernel=E.KERNEL_PLAIN, step_cap=50, batch=3)])
+def test_tunings_do_not_change_results(searches, tune):
+    e = searches["local_edits_f2"]
+    per_x, lines = run_entry(e, E.tuning(**tune))
+    check_entry(e, per_x)
+    assert lines == golden_lines(e)
+
+
+def test_base_and_mutants():
+    import os
+    gold = os.path.join(os.path.dirname(__file__), "golden")
+    base = O.load_machine("erdos_14.txt")
+    tabs, keys = [], []
+    for i in range(28):
+        for v in range(-1, 56):
+            if v == base[i]:
+                continue
+            t = list(base)
+            t[i] = v
+            tabs.append(t)
+            keys.append((i, v))
+    out = ctx().run_full([base] + tabs, 14)
+    r = out[0]
+    assert r == [1, 9, 2, -2, 1, 0, 208864]
+    got = [f"{i} {v} {o[1]} {o[0]}" for (i, v), o in zip(keys, out[1:])]
+    exp = [l.rstrip("\n") for l in open(os.path.join(gold, "mutants.txt")) if l.strip() and not l.startswith("#")]
+    assert got == exp
+
+
+def test_survivor_cap_reports_overflow(searches):
+    e = searches["split_test"]
+    job = __import__("gpu_common").make_job(e, 14)
+    c, surv = ctx().search(job, None, surv_cap=1)
+    assert c.survivors == 3 and len(surv) == 1

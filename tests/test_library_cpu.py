@@ -1,0 +1,104 @@
+"""libe13b200.so without a GPU: it loads, exports every entry point that
+include/e13.h declares, and its host-side helpers (keys, machine files,
+candidate setup, text formats) agree with the oracle and the reference's
+formats.  No compute call is made here."""
+import os
+import re
+
+import pytest
+
+import e13b200 as E
+import oracle_lib as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "e13.h")).read()
+    return sorted(set(re.findall(r"\b(e13_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = E.lib()
+    for name in declared_symbols():
+        assert hasattr(L, name), name
+    assert set(declared_symbols()) >= set(E.EXPORTED)
+
+
+def test_keys_equal_oracle():
+    assert E.keys() == O.keys()
+
+
+def test_machine_parsing():
+    path = os.path.join(O.MACHINES, "erdos_14.txt")
+    assert E.load_machine(path) == O.load_machine("erdos_14.txt")
+    assert E.parse_machine(open(path).read()) == O.load_machine("erdos_14.txt")
+    with pytest.raises(E.E13Error):
+        E.load_machine("/nonexistent/machine.txt")
+
+
+@pytest.mark.parametrize("machine", ["erdos_14.txt", "split_15.txt", "counters_3state/base_07.txt"])
+def test_setup_delete_matches_oracle(machine):
+    base = O.load_machine(machine)
+    nq0 = len(base) // 2
+    for X in range(-1, nq0):
+        for fmax in (0, 1, 2, 4):
+            r, job = E.setup(base, X, fmax=fmax)
+            ro, jo = O.setup(base, X, fmax=fmax)
+            if ro == -1:
+                assert r == -2
+                continue
+            assert r == 0 and job.budget == ro
+            assert list(job.tab)[: 2 * job.nq] == jo.tab
+            assert job.nforced == jo.nforced
+
+
+@pytest.mark.parametrize("X,lo,hi,free", [
+    (13, 10, 13, ["D0", "G0", "K0", "K1", "L1", "M1"]),
+    (9, 3, 9, ["F0", "F1", "G0", "G1", "H0", "H1", "I0", "I1"]),
+    (9, 3, 9, ["F0", "F1"]),
+    (13, 0, 13, ["A0", "A1"]),
+    (2, -1, -1, ["A0", "A1", "B0", "B1"]),
+])
+def test_setup_free_matches_oracle(X, lo, hi, free):
+    base = O.load_machine("erdos_14.txt")
+    r, job = E.setup(base, X, free_cells=free, lo=lo, hi=hi)
+    ro, jo = O.setup(base, X, free_cells=free, lo=lo, hi=hi)
+    assert r == (0 if ro >= 0 else ro)
+    if r == 0:
+        assert list(job.tab)[: 2 * job.nq] == jo.tab
+        assert (job.sym_lo, job.sym_hi, job.sym_n0) == (jo.sym_lo, jo.sym_hi, jo.sym_n0)
+
+
+def test_format_survivor_matches_reference_text():
+    line = open(os.path.join(os.path.dirname(__file__), "golden", "surv", "f2.txt")).read().strip()
+    ci = E.parse_survivor_line(line)
+    assert ci is not None and ci.nq == 13
+    # rebuild the survivor record from the line and format it back
+    base = O.load_machine("erdos_14.txt")
+    _, job = E.setup(base, 8, fmax=2)
+    s = E.Survivor()
+    for i in range(26):
+        s.tab[i] = -1 if ci.kind[i] else (ci.next[i] << 2) | ((ci.move[i] > 0) << 1) | ci.write[i]
+    s.read_mask = (1 << 26) - 1
+    s.st0, s.head0, s.abs_ok, s.rel_ok, s.steps = 2, -2, 1, 0, 208838
+    assert E.survivor_line(job, s) == line
+
+
+def test_summary_format():
+    base = O.load_machine("erdos_14.txt")
+    _, job = E.setup(base, 9, free_cells=["F0", "F1", "G0", "G1", "H0", "H1", "I0", "I1"], lo=3, hi=9)
+    c = E.Counts(830955779, 0, 96702705048, (E.ctypes.c_uint64 * 10)(0, 755283390, 74755943, 852182, 20270, 420,
+                                                                         36, 0, 43538, 0))
+    line = E.summary_line(job, c, 1.0)
+    assert O.parse_summary(line) == dict(X=9, leaves=830955779, survivors=0, steps=96702705048,
+                                         hist=[0, 755283390, 74755943, 852182, 20270, 420, 36, 0, 43538, 0])
+
+
+def test_no_device_is_an_error_not_a_fallback():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(E.E13Error) as ei:
+        E.Context(0)
+    assert ei.value.code in (-11, -5)
