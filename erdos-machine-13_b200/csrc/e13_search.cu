@@ -79,7 +79,7 @@ __device__ __forceinline__ void lane_load(Lane &L, const Node *N, u32 *tcol, u32
   L.tgt = c_tgt[L.nt];
   L.tseg = L.t;
   const u32 *e32 = reinterpret_cast<const u32 *>(N->ent);
-  for (int k = 0; 2 * k < nq; ++k) {
+  for (int k = 0; k < 8; ++k) {  // all 16 rows: states >= nq hold halts
     const u32 w = e32[k];
     rcol[(2 * k) * stride] = __byte_perm(w, 0u, 0x4140);
     rcol[(2 * k + 1) * stride] = __byte_perm(w, 0u, 0x4342);
@@ -108,11 +108,7 @@ __device__ __forceinline__ void lane_store(const Lane &L, Node *N, const u32 *tc
   N->nintro = (unsigned char)L.nintro;
   N->budget = (unsigned char)L.budget;
   u32 *e32 = reinterpret_cast<u32 *>(N->ent);
-  for (int k = 0; 2 * k < nq; ++k) {
-    const u32 r0 = rcol[(2 * k) * stride];
-    const u32 r1 = (2 * k + 1 < 16) ? rcol[(2 * k + 1) * stride] : 0u;
-    e32[k] = __byte_perm(r0, r1, 0x6420);
-  }
+  for (int k = 0; k < 8; ++k) e32[k] = __byte_perm(rcol[(2 * k) * stride], rcol[(2 * k + 1) * stride], 0x6420);
   int lo, hi;
   tape_extent(L.t, lo, hi);
   for (int w = lo; w <= hi; ++w) N->tape[w] = tcol[w * stride];
@@ -464,10 +460,11 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
 
 // Between launches: the input taken from the top of the stack is gone; the
 // outputs go where it was.
-__global__ void move_outputs(Ctl *ctl, Node *stack, const Node *out) {
+__global__ void move_outputs(Ctl *ctl, Node *stack, const Node *out, long long cap) {
   const long long used = min((long long)ctl->cursor, ctl->batch);
   const long long base = ctl->top - used;
   const long long n = (long long)ctl->nout;
+  if (base + n > cap || ctl->error) return;  // finish_launch reports the overflow
   const long long chunks = n * kNodeChunks;
   uint4 *dst = reinterpret_cast<uint4 *>(stack + base);
   const uint4 *src = reinterpret_cast<const uint4 *>(out);
@@ -478,6 +475,11 @@ __global__ void move_outputs(Ctl *ctl, Node *stack, const Node *out) {
 __global__ void finish_launch(Ctl *ctl, long long cap, long long batch_max) {
   const long long used = min((long long)ctl->cursor, ctl->batch);
   long long top = ctl->top - used + (long long)ctl->nout;
+  if (top > cap || ctl->error) {
+    // the outputs did not fit: stop the search here and let the host report it
+    ctl->error |= kErrOverflow;
+    top = 0;
+  }
   ctl->top = top;
   if (top > ctl->peak) ctl->peak = top;
   ctl->batch = min(top, batch_max);
@@ -700,6 +702,8 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   if (!c || !job || !counts || !nsurv || (surv_cap > 0 && !surv) || surv_cap < 0) return E13_ERR_ARG;
   if (job->nq < 1 || job->nq > 16) return E13_ERR_NQ;
   if (job->budget < 0) return E13_ERR_FMAX;
+  for (int i = 0; i < 2 * job->nq; ++i)
+    if (job->tab[i] < E13_FREE || (job->tab[i] >= 0 && (job->tab[i] >> 2) >= job->nq)) return E13_ERR_ARG;
   e13_tuning tu;
   e13_default_tuning(&tu);
   if (tuning) {
@@ -784,7 +788,7 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     for (int e = 0; e < tu.epochs_per_graph; ++e) {
       search_kernel<true><<<blocks, tu.block, smem, c->stream>>>(P);
-      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out);
+      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->stack_cap);
       finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, batch_max);
     }
     CK(cudaStreamEndCapture(c->stream, &graph));
@@ -810,7 +814,7 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   } else {
     for (;;) {
       search_kernel<false><<<blocks, tu.block, smem, c->stream>>>(P);
-      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out);
+      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->stack_cap);
       finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, batch_max);
       launches += 3;
       search_launches += 1;
