@@ -1,1 +1,171 @@
-int main(void){return 0;}
+/* e13search -- drop-in for the reference's e13search (src/e13search.c:25-45,
+   435-513) on one B200, over the C-ABI of libe13b200.so.
+
+     e13search base   machine.txt
+     e13search mutant machine.txt
+     e13search delete machine.txt FMAX X...
+     e13search free machine.txt X CELL...
+     e13search freesym machine.txt X LO HI CELL...
+
+   Survivors go to stdout in the reference's format, one summary line per X to
+   stderr.  Environment: E13_DEVICE (CUDA device, default 0), E13_KERNEL
+   (persistent | plain).  There is no CPU path: without a GPU it exits 1. */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include "e13.h"
+
+static double now_s(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+static e13_ctx *open_ctx(void) {
+  const char *d = getenv("E13_DEVICE");
+  e13_ctx *ctx = NULL;
+  int rc = e13_ctx_create(d ? atoi(d) : 0, &ctx);
+  if (rc) {
+    fprintf(stderr, "e13search: no usable CUDA device (error %d)\n", rc);
+    exit(1);
+  }
+  return ctx;
+}
+
+static int run_one(e13_ctx *ctx, const e13_job *job, const e13_tuning *tu) {
+  int cap = 1 << 16;
+  e13_survivor *surv = (e13_survivor *)malloc(sizeof(e13_survivor) * (size_t)cap);
+  e13_counts c;
+  int ns = 0;
+  double w0 = now_s();
+  int rc = e13_search(ctx, job, tu, &c, surv, cap, &ns);
+  double wall = now_s() - w0;
+  if (rc && rc != E13_ERR_SURV_CAP) {
+    fprintf(stderr, "X=%d search failed (error %d)\n", job->X, rc);
+    free(surv);
+    return rc;
+  }
+  char line[2048];
+  int shown = ns < cap ? ns : cap;
+  for (int i = 0; i < shown; i++) {
+    e13_format_survivor(job, &surv[i], line, sizeof line);
+    printf("%s\n", line);
+  }
+  fflush(stdout);
+  e13_format_summary(job, &c, wall, line, sizeof line);
+  fprintf(stderr, "%s\n", line);
+  if (rc == E13_ERR_SURV_CAP) fprintf(stderr, "WARNING: %d survivors, only %d printed\n", ns, cap);
+  fflush(stderr);
+  free(surv);
+  return 0;
+}
+
+int main(int argc, char **argv) {
+  if (argc < 3) {
+    fprintf(stderr, "usage: e13search base|mutant|delete|free|freesym machine.txt [FMAX X...]\n");
+    return 1;
+  }
+  int32_t base[E13_MAXCELLS];
+  int nq0 = e13_load_machine(argv[2], base);
+  if (nq0 < 0) {
+    fprintf(stderr, "cannot open %s\n", argv[2]);
+    return 1;
+  }
+  e13_tuning tu;
+  e13_default_tuning(&tu);
+  const char *k = getenv("E13_KERNEL");
+  if (k && !strcmp(k, "plain")) tu.kernel = E13_KERNEL_PLAIN;
+  const char *mode = argv[1];
+
+  if (!strcmp(mode, "base") || !strcmp(mode, "mutant")) {
+    e13_ctx *ctx = open_ctx();
+    if (!strcmp(mode, "base")) {
+      int64_t o[7];
+      if (e13_run_full(ctx, base, 1, nq0, o)) return 1;
+      printf("base states=%d result=%s stage=%lld st0=%lld head0=%lld abs=%lld rel=%lld steps=%lld\n", nq0,
+             o[0] ? "SURV" : "DEAD", (long long)o[1], (long long)o[2], (long long)o[3], (long long)o[4],
+             (long long)o[5], (long long)o[6]);
+    } else {
+      int n = 0, cap = 2 * nq0 * (4 * nq0 + 1);
+      int32_t *tabs = (int32_t *)malloc(sizeof(int32_t) * E13_MAXCELLS * (size_t)cap);
+      int *cell = (int *)malloc(sizeof(int) * (size_t)cap), *val = (int *)malloc(sizeof(int) * (size_t)cap);
+      for (int i = 0; i < 2 * nq0; i++)
+        for (int v = -1; v < 4 * nq0; v++) {
+          if (v == base[i]) continue;
+          memcpy(tabs + (size_t)n * E13_MAXCELLS, base, sizeof(int32_t) * E13_MAXCELLS);
+          tabs[(size_t)n * E13_MAXCELLS + i] = v;
+          cell[n] = i;
+          val[n] = v;
+          n++;
+        }
+      int64_t *o = (int64_t *)malloc(sizeof(int64_t) * 7 * (size_t)n);
+      if (e13_run_full(ctx, tabs, n, nq0, o)) return 1;
+      for (int j = 0; j < n; j++)
+        printf("%d %d %lld %lld\n", cell[j], val[j], (long long)o[7 * j + 1], (long long)o[7 * j]);
+      free(tabs);
+      free(cell);
+      free(val);
+      free(o);
+    }
+    e13_ctx_destroy(ctx);
+    return 0;
+  }
+  if (!strcmp(mode, "delete")) {
+    if (argc < 5) return 1;
+    int fmax = atoi(argv[3]);
+    e13_ctx *ctx = open_ctx();
+    for (int i = 4; i < argc; i++) {
+      e13_job job;
+      int X = atoi(argv[i]);
+      int rc = e13_setup(base, nq0, X, fmax, NULL, -1, -1, &job);
+      if (rc == E13_ERR_FMAX) {
+        fprintf(stderr, "X=%d forced=%d > fmax\n", X, job.nforced);
+        continue;
+      }
+      if (rc) {
+        fprintf(stderr, "X=%d: setup error %d\n", X, rc);
+        return 1;
+      }
+      if (run_one(ctx, &job, &tu)) return 1;
+    }
+    e13_ctx_destroy(ctx);
+    return 0;
+  }
+  if (!strcmp(mode, "free") || !strcmp(mode, "freesym")) {
+    if (argc < 4) return 1;
+    uint8_t freebase[E13_MAXCELLS] = {0};
+    int X = atoi(argv[3]), a0 = 4, lo = -1, hi = -1;
+    if (!strcmp(mode, "freesym")) {
+      if (argc < 6) return 1;
+      lo = atoi(argv[4]);
+      hi = atoi(argv[5]);
+      a0 = 6;
+    }
+    for (int i = a0; i < argc; i++) {
+      int c = 2 * (argv[i][0] - 'A') + (argv[i][1] - '0');
+      if (c >= 0 && c < E13_MAXCELLS) freebase[c] = 1;
+    }
+    e13_job job;
+    int rc = e13_setup(base, nq0, X, 0, freebase, lo, hi, &job);
+    if (rc == E13_ERR_SYM_NAMED) {
+      fprintf(stderr, "symmetric state is named by a fixed cell or has one\n");
+      return 1;
+    }
+    if (rc == E13_ERR_SYM_START) {
+      fprintf(stderr, "start state in the symmetric states\n");
+      return 1;
+    }
+    if (rc) {
+      fprintf(stderr, "setup error %d\n", rc);
+      return 1;
+    }
+    e13_ctx *ctx = open_ctx();
+    rc = run_one(ctx, &job, &tu);
+    e13_ctx_destroy(ctx);
+    return rc ? 1 : 0;
+  }
+  fprintf(stderr, "unknown mode %s\n", mode);
+  return 1;
+}
