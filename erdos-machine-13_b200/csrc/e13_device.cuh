@@ -2,7 +2,7 @@
 // whole-table runner and the survivor checker of libe13b200.so (sm_100a).
 //
 // One Turing machine per lane.  A lane's tape (1364 cells, bit-packed into 43
-// words) and its table (16 rows of two 8-bit cell entries) live in shared
+// words) and its table (16 rows of two 16-bit cell slots) live in shared
 // memory, interleaved by lane: word w of lane l sits at [w * blockDim + l], so
 // every lane always hits its own bank and a warp-wide access never conflicts.
 //
@@ -28,6 +28,10 @@ constexpr u32 kEntHalt = 0x40;    // halt
 constexpr u32 kEntUnread = 0x80;  // never read yet: the first read is an event
 constexpr u32 kEntFree = 0xFF;    // free cell, no move yet (FORCED, src/e13search.c:66)
 constexpr u32 kEntSpecial = 0xC0; // any of the above: leaves the fast path
+// Bit 8 of a cell's 16-bit slot in a row: the cell is a read self-loop (next
+// state = this state, writes the symbol it reads), so the head sweeps a run of
+// that symbol; the step loop then advances over the run a word at a time.
+constexpr u32 kEntSelf = 0x100;
 
 // Node flags byte.
 constexpr int kFlagAbs = 1, kFlagRel = 2, kFlagCs0 = 4, kFlagKeep = 32;
@@ -44,9 +48,9 @@ struct __align__(16) Node {
   short p0, pend;
   unsigned char nintro, budget, pad0, pad1;
   u32 pad2;
-  unsigned char ent[32];
+  unsigned short cellv[32];  // cell entries with the self-loop bit; row s = cellv[2s] | cellv[2s+1] << 16
   u32 tape[kTapeWords];
-  u32 pad3;
+  u32 pad3[5];
 };
 static_assert(sizeof(Node) % 16 == 0, "Node must be a whole number of 16-byte chunks");
 constexpr int kNodeChunks = sizeof(Node) / 16;
@@ -101,11 +105,46 @@ __device__ __forceinline__ void tape_extent(int t, int &lo, int &hi) {
   hi = b >> 5;
 }
 
+// Length of the run of `sym` cells starting at p in the move direction, at
+// most lim (lim >= 1; cell p itself holds sym).
+__device__ __forceinline__ int run_length(const u32 *__restrict__ tcol, int stride, int p, u32 sym, bool right,
+                                          int lim) {
+  const u32 flip = sym ? 0xFFFFFFFFu : 0u;  // after the XOR, cells holding sym are 0 bits
+  int w = p >> 5, b = p & 31, k = 0;
+  if (right) {
+    u32 x = (tcol[w * stride] ^ flip) >> b;
+    for (;;) {
+      k += x ? (__ffs(x) - 1) : (32 - b);
+      if (x || k >= lim || w == kTapeWords - 1) break;
+      ++w;
+      b = 0;
+      x = tcol[w * stride] ^ flip;
+    }
+  } else {
+    u32 x = (tcol[w * stride] ^ flip) << (31 - b);
+    for (;;) {
+      k += x ? __clz(x) : (b + 1);
+      if (x || k >= lim || w == 0) break;
+      --w;
+      b = 31;
+      x = tcol[w * stride] ^ flip;
+    }
+  }
+  return k < lim ? k : lim;
+}
+
 // Runs up to n steps.  Returns kEvRun when n is used up, else the event that
 // stopped it; the lane is then exactly at the reference's state for that event.
 // The stage test of the current configuration has already been done on entry
 // (re-running it at the same configuration changes nothing, as the reference
 // notes at src/e13search.c:131-133).
+//
+// Run skip: on a self-loop cell the next k steps read the same symbol, write
+// nothing and keep the state, so hb stays the same; when hb != TGT[nt] no stage
+// test can fire inside the run.  k is clamped so that every skipped step would
+// also have passed the deadline test (t + i <= deadline) and the window test
+// (the head stays in 1..1362); the step that fails either test is then taken by
+// the normal loop.  Steps counted and the death point equal single-stepping.
 __device__ __forceinline__ int step_slice(int &p, int &st, int &t, const int deadline, u64 &hb, const u64 tgt,
                                           u32 *__restrict__ tcol, const u32 *__restrict__ rcol,
                                           const u64 *__restrict__ keyb, const int stride, int &n, int &cell) {
@@ -115,10 +154,28 @@ __device__ __forceinline__ int step_slice(int &p, int &st, int &t, const int dea
     const u32 word = tcol[widx];
     const u32 row = rcol[st * stride];
     const u32 sym = (word >> (p & 31)) & 1u;
-    const u32 e = (row >> (sym << 4)) & 0xFFu;
-    if (e & kEntSpecial) {
-      cell = (st << 1) | (int)sym;
-      return kEvCell;
+    const u32 e = (row >> (sym << 4)) & 0x1FFu;
+    if (e & (kEntSpecial | kEntSelf)) {
+      if (e & kEntSpecial) {
+        cell = (st << 1) | (int)sym;
+        return kEvCell;
+      }
+      if (hb != tgt) {
+        const bool right = (e & 2u) != 0;
+        int lim = deadline - t + 1;
+        lim = lim < n ? lim : n;
+        const int room = right ? (kTapeCells - 2) - p : p - 1;
+        lim = lim < room ? lim : room;
+        if (lim > 1) {
+          const int k = run_length(tcol, stride, p, sym, right, lim);
+          if (k > 1) {
+            p += right ? k : -k;
+            t += k;
+            n -= k;
+            continue;
+          }
+        }
+      }
     }
     if ((e ^ sym) & 1u) {
       tcol[widx] = word ^ (1u << (p & 31));
@@ -126,7 +183,7 @@ __device__ __forceinline__ int step_slice(int &p, int &st, int &t, const int dea
     }
     p += (int)(e & 2u) - 1;
     if ((unsigned)(p - 1) >= (unsigned)(kTapeCells - 2)) return kEvDead;  // head <= -64 or >= 1299
-    st = (int)(e >> 2);
+    st = (int)((e >> 2) & 15u);
     ++t;
     --n;
     if (hb == tgt) return kEvStage;
@@ -188,10 +245,17 @@ __device__ __forceinline__ u32 get_entry(const u32 *rcol, int stride, int cell) 
   return (rcol[(cell >> 1) * stride] >> ((cell & 1) << 4)) & 0xFFu;
 }
 
-__device__ __forceinline__ void set_entry(u32 *rcol, int stride, int cell, u32 v) {
+// The 16-bit slot of a cell holding entry v, with the self-loop bit when
+// run_skip is on and v is a read move that keeps the state and the symbol.
+__device__ __forceinline__ u32 cell_slot(int cell, u32 v, bool run_skip) {
+  const bool self = run_skip && v < 64u && (int)(v >> 2) == (cell >> 1) && (int)(v & 1u) == (cell & 1);
+  return v | (self ? kEntSelf : 0u);
+}
+
+__device__ __forceinline__ void set_entry(u32 *rcol, int stride, int cell, u32 v, bool run_skip) {
   u32 *w = rcol + (cell >> 1) * stride;
   const int sh = (cell & 1) << 4;
-  *w = (*w & ~(0xFFu << sh)) | (v << sh);
+  *w = (*w & ~(0xFFFFu << sh)) | (cell_slot(cell, v, run_skip) << sh);
 }
 
 // Relabel symmetry (src/e13search.c:206-212): states in use after move v, or

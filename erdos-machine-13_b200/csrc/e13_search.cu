@@ -42,7 +42,7 @@ constexpr int kKeySmemBytes = (kTapeCells + 64) * 8;
 
 struct Params {
   int nq, nv, sym_lo, sym_hi;
-  int slice, step_cap, wdepth, starve_limit;
+  int slice, step_cap, wdepth, starve_limit, run_skip;
   long long out_cap, out_soft, surv_cap;
   long long epoch_ns;
   Node *stack, *out, *wstack;
@@ -78,11 +78,13 @@ __device__ __forceinline__ void lane_load(Lane &L, const Node *N, u32 *tcol, u32
   L.budget = N->budget;
   L.tgt = c_tgt[L.nt];
   L.tseg = L.t;
-  const u32 *e32 = reinterpret_cast<const u32 *>(N->ent);
-  for (int k = 0; k < 8; ++k) {  // all 16 rows: states >= nq hold halts
-    const u32 w = e32[k];
-    rcol[(2 * k) * stride] = __byte_perm(w, 0u, 0x4140);
-    rcol[(2 * k + 1) * stride] = __byte_perm(w, 0u, 0x4342);
+  const uint4 *rv = reinterpret_cast<const uint4 *>(N->cellv);
+  for (int k = 0; k < 4; ++k) {  // all 16 rows: states >= nq hold halts
+    const uint4 v = rv[k];
+    rcol[(4 * k) * stride] = v.x;
+    rcol[(4 * k + 1) * stride] = v.y;
+    rcol[(4 * k + 2) * stride] = v.z;
+    rcol[(4 * k + 3) * stride] = v.w;
   }
   tape_extent(L.t, lo, hi);
   for (int w = lo; w <= hi; ++w) tcol[w * stride] = N->tape[w];
@@ -107,8 +109,10 @@ __device__ __forceinline__ void lane_store(const Lane &L, Node *N, const u32 *tc
   N->pend = (short)pend;
   N->nintro = (unsigned char)L.nintro;
   N->budget = (unsigned char)L.budget;
-  u32 *e32 = reinterpret_cast<u32 *>(N->ent);
-  for (int k = 0; k < 8; ++k) e32[k] = __byte_perm(rcol[(2 * k) * stride], rcol[(2 * k + 1) * stride], 0x6420);
+  uint4 *rv = reinterpret_cast<uint4 *>(N->cellv);
+  for (int k = 0; k < 4; ++k)
+    rv[k] = make_uint4(rcol[(4 * k) * stride], rcol[(4 * k + 1) * stride], rcol[(4 * k + 2) * stride],
+                       rcol[(4 * k + 3) * stride]);
   int lo, hi;
   tape_extent(L.t, lo, hi);
   for (int w = lo; w <= hi; ++w) N->tape[w] = tcol[w * stride];
@@ -117,16 +121,16 @@ __device__ __forceinline__ void lane_store(const Lane &L, Node *N, const u32 *tc
 // Applies child `ch` (-1: keep / go on, else move v) of node N to a lane that
 // has just loaded N.
 __device__ __forceinline__ void apply_child(Lane &L, const Node *N, int ch, u32 *rcol, int stride, int sym_lo,
-                                            int sym_hi) {
+                                            int sym_hi, bool run_skip) {
   const int pend = N->pend;
   if (pend < 0) return;
-  const u32 e = N->ent[pend];
+  const u32 e = N->cellv[pend] & 0xFFu;
   if (ch < 0) {
-    set_entry(rcol, stride, pend, e & 0x7Fu);  // the table's own move (or halt), now read
+    set_entry(rcol, stride, pend, e & 0x7Fu, run_skip);  // the table's own move (or halt), now read
   } else {
     if (e != kEntFree) L.budget -= 1;
     L.nintro = sym_after(ch, L.nintro, sym_lo, sym_hi);
-    set_entry(rcol, stride, pend, (u32)ch);
+    set_entry(rcol, stride, pend, (u32)ch, run_skip);
   }
 }
 
@@ -139,11 +143,7 @@ __device__ __forceinline__ void record_survivor(const Params &P, const Lane &L, 
   if ((long long)k >= P.surv_cap) return;
   SurvRec *r = P.surv + k;
   u32 *e32 = reinterpret_cast<u32 *>(r->ent);
-  for (int k2 = 0; k2 < 8; ++k2) {
-    const u32 r0 = (2 * k2 < P.nq) ? rcol[(2 * k2) * stride] : 0xC0C0u;
-    const u32 r1 = (2 * k2 + 1 < P.nq) ? rcol[(2 * k2 + 1) * stride] : 0xC0C0u;
-    e32[k2] = __byte_perm(r0, r1, 0x6420);
-  }
+  for (int k2 = 0; k2 < 8; ++k2) e32[k2] = __byte_perm(rcol[(2 * k2) * stride], rcol[(2 * k2 + 1) * stride], 0x6420);
   r->st0 = L.st0;
   r->head0 = L.p0 - kLeft;
   r->abs_ok = L.flags & 1;
@@ -257,11 +257,11 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
         if (status == kStFork) {
           // the fork's own state becomes its first child, in place
           if (first < 0) {
-            set_entry(rcol, stride, fork_cell, fork_e & 0x7Fu);
+            set_entry(rcol, stride, fork_cell, fork_e & 0x7Fu, P.run_skip);
           } else {
             if (fork_e != kEntFree) L.budget -= 1;
             L.nintro = sym_after(first, L.nintro, P.sym_lo, P.sym_hi);
-            set_entry(rcol, stride, fork_cell, (u32)first);
+            set_entry(rcol, stride, fork_cell, (u32)first, P.run_skip);
           }
           status = kStRun;
         }
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
         int ch = -1;
         if (!(cur_keep && rank == 0)) ch = nth_bit64(cur_vm, rank - cur_keep);
         lane_load(L, N, tcol, rcol, stride, P.nq);
-        apply_child(L, N, ch, rcol, stride, P.sym_lo, P.sym_hi);
+        apply_child(L, N, ch, rcol, stride, P.sym_lo, P.sym_hi, P.run_skip);
         status = kStRun;
       }
       __syncwarp();
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
             break;
           } else {
             // first read with nothing to branch on: the cell is now fixed
-            set_entry(rcol, stride, cell, e & 0x7Fu);
+            set_entry(rcol, stride, cell, e & 0x7Fu, P.run_skip);
             if ((e & 0x7Fu) == kEntHalt) ev = kEvDead;
             else continue;
           }
@@ -513,7 +513,7 @@ __global__ void __launch_bounds__(256) run_full_kernel(const int *tabs, int n, i
       e0 = tab[2 * s] < 0 ? kEntHalt : (u32)tab[2 * s];
       e1 = tab[2 * s + 1] < 0 ? kEntHalt : (u32)tab[2 * s + 1];
     }
-    rcol[s * stride] = e0 | (e1 << 16);
+    rcol[s * stride] = cell_slot(2 * s, e0, true) | (cell_slot(2 * s + 1, e1, true) << 16);
   }
   Lane L;
   L.p = kLeft; L.st = 0; L.t = 0; L.deadline = c_deadline[1]; L.hb = 0; L.tgt = c_tgt[1];
@@ -671,7 +671,7 @@ static void build_root(const e13_job *job, Node *root) {
       else if (c < 0) e = (unsigned char)(kEntUnread | kEntHalt);
       else e = (unsigned char)(kEntUnread | (unsigned)c);
     }
-    root->ent[i] = e;
+    root->cellv[i] = e;
   }
 }
 
@@ -751,6 +751,7 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   P.sym_lo = job->sym_lo;
   P.sym_hi = job->sym_hi;
   P.slice = tu.slice;
+  P.run_skip = tu.run_skip ? 1 : 0;
   P.step_cap = tu.step_cap;
   P.wdepth = tu.warp_stack;
   P.starve_limit = (int)std::max<long long>(1, nwarps * tu.starve_pct / 100);

@@ -64,5 +64,6 @@ def test_deep15_v1_sample():
     idx = list(range(0, 2868, 97))
     ins = [E.parse_survivor_line(lines[i]) for i in idx]
     outs = ctx().check(ins, 15, 1)
+    # the golden file was made in chunks whose ids restart: compare the text after the id
     for i, ci, o in zip(idx, ins, outs):
-        assert f"survivor {i + 1} " + E.format_deep(ci, o, 15) == exp[i]
+        assert E.format_deep(ci, o, 15) == exp[i].split(" ", 2)[2]

@@ -141,3 +141,14 @@ def test_survivor_cap_reports_overflow(searches):
     job = __import__("gpu_common").make_job(e, 14)
     c, surv = ctx().search(job, None, surv_cap=1)
     assert c.survivors == 3 and len(surv) == 1
+
+
+@pytest.mark.parametrize("name", ["local_edits_f2", "split_test_free", "counters_f2_base_07"])
+def test_run_skip_is_exact(searches, name):
+    """Advancing whole words across a self-loop run gives the same counts,
+    steps and survivors as single steps."""
+    e = searches[name]
+    a = run_entry(e, E.tuning(run_skip=0))
+    b = run_entry(e, E.tuning(run_skip=1))
+    assert a == b
+    check_entry(e, b[0])
