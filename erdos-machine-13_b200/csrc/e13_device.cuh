@@ -70,13 +70,17 @@ struct Ctl {
   long long peak;
   unsigned long long nsurv;      // survivors found (records kept: min(nsurv, cap))
   int dump;                      // persistent: end the epoch now
-  int starved;                   // persistent: warps out of work
+  int busy;                      // persistent: warps holding work or claiming it
   int error;                     // kErr* bits
   int launches;
   u64 leaves, steps;
   u64 hist[kStages + 1];
+  // persistent: nodes donated by warps with deep stacks to warps without work
+  // (slots [pool_head, pool_tail) are waiting; each counter on its own cache line)
+  alignas(128) unsigned long long pool_head;
+  alignas(128) unsigned long long pool_tail;
 };
-constexpr int kErrOverflow = 1, kErrOutFull = 2;
+constexpr int kErrOverflow = 1, kErrOutFull = 2, kErrTimeout = 4;
 
 // The filter's constant tables (set by the host from e13_keys()).
 __constant__ u64 c_key[kTapeCells];

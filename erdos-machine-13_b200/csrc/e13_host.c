@@ -164,9 +164,9 @@ void e13_default_tuning(e13_tuning *t) {
   t->warp_stack = 64;
   t->step_cap = 20000;
   t->batch = 0;
-  t->epoch_us = 200000;
-  t->epochs_per_graph = 8;
-  t->starve_pct = 25;
+  t->epoch_us = 500000;
+  t->epochs_per_graph = 4;
+  t->pool_low_pct = 25;
   t->run_skip = 1;
   t->stack_nodes = 0;
 }

@@ -11,9 +11,11 @@
 //  * persistent (PERSIST = true): each warp runs a private depth-first search
 //    over the subtrees it pulls.  A forking lane pushes its node on the warp's
 //    stack and goes on with the first child in place (no copy); idle lanes take
-//    the next children of the stack top at the next round.  An epoch ends when
-//    enough warps starve or a time bound passes: warps then dump live lanes and
-//    stack nodes back to the frontier, and the next epoch rebalances.  Epochs
+//    the next children of the stack top at the next round.  A warp whose stack
+//    is deep donates its oldest node to a device pool when the pool runs low;
+//    warps without work take pool nodes.  An epoch ends on a time bound (or
+//    when every warp is out of work): warps then dump live lanes and stack
+//    nodes back to the frontier.  Epochs
 //    are replayed from a captured CUDA graph; the host reads the control block
 //    once per graph.
 //
@@ -37,15 +39,17 @@ namespace {
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kMaxBlock = 896;
 constexpr int kKeySmemBytes = (kTapeCells + 64) * 8;
+constexpr long long kPoolNodes = 1LL << 18;  // donation pool: 256 Ki nodes (80 MiB)
 
 // steps a lane gets between warp-level refill rounds is Params::slice
 
 struct Params {
   int nq, nv, sym_lo, sym_hi;
-  int slice, step_cap, wdepth, starve_limit, run_skip;
-  long long out_cap, out_soft, surv_cap;
+  int slice, step_cap, wdepth, pool_low, run_skip;
+  long long out_cap, out_soft, surv_cap, pool_cap;
   long long epoch_ns;
-  Node *stack, *out, *wstack;
+  Node *stack, *out, *wstack, *pool;
+  int *pool_ready;
   SurvRec *surv;
   Ctl *ctl;
 };
@@ -153,6 +157,13 @@ __device__ __forceinline__ void record_survivor(const Params &P, const Lane &L, 
 
 enum { kStRun = 0, kStIdle = 1, kStFork = 2, kStCap = 3 };
 
+__device__ __forceinline__ void copy_node_cg(Node *dst, const Node *src, int lane) {
+  // a pool node written by another SM: read past L1
+  if (lane < kNodeChunks) reinterpret_cast<uint4 *>(dst)[lane] = __ldcg(reinterpret_cast<const uint4 *>(src) + lane);
+}
+
+__device__ __forceinline__ int wrap(int s, int d) { return s >= d ? s - d : s; }
+
 template <bool PERSIST>
 __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -182,7 +193,9 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   Ctl *ctl = P.ctl;
   const long long top0 = ctl->top;
   const long long batch = ctl->batch;
-  Node *wst = PERSIST ? P.wstack + gwarp * P.wdepth : nullptr;
+  const int tag = ctl->launches + 1;  // marks pool slots written in this launch
+  const int D = P.wdepth;
+  Node *wst = PERSIST ? P.wstack + gwarp * D : nullptr;
   const unsigned long long t_begin = PERSIST ? globaltimer() : 0ull;
 
   Lane L;
@@ -195,14 +208,15 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   unsigned long long steps = 0;
 
   // warp-uniform state
-  int sp = 0;                  // persistent: nodes on this warp's stack
-  bool have_cur = false;       // a node whose children are being handed out
-  const Node *cur = nullptr;   // plain: that node (in the input)
+  int sp = 0, wbot = 0;        // persistent: this warp's DFS stack, a ring of D slots from wbot
+  bool have_cur = false;       // cursor registers hold the children left of the current node
+  const Node *cur = nullptr;   // plain: the current input node
   int cur_keep = 0;
   u64 cur_vm = 0;
   bool input_done = false;
-  bool counted_starve = false;
+  bool busy = false;           // persistent: counted in ctl->busy
   int rounds = 0;              // slices run: a warp dumps only after one (progress every epoch)
+  unsigned backoff = 256;
 
   for (;;) {
     // ---- (A) forks
@@ -211,7 +225,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
       u64 vm = 0;
       if (status == kStFork) child_set(fork_e, L.budget, L.nintro, P.nv, P.sym_lo, P.sym_hi, keep, vm);
       if (PERSIST) {
-        // the forking lane goes on with the first child; the rest is pushed
+        // the forking lane goes on with the first child in place; the rest is pushed
         int first = -2;
         if (status == kStFork) {
           if (keep) {
@@ -226,16 +240,17 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
         const unsigned pm = __ballot_sync(kFull, more);
         if (pm) {
           if (have_cur && sp > 0 && lane == 0) {
-            wst[sp - 1].vmask = cur_vm;
-            wst[sp - 1].flags = (signed char)((wst[sp - 1].flags & 31) | (cur_keep ? kFlagKeep : 0));
+            Node *t = wst + wrap(wbot + sp - 1, D);
+            t->vmask = cur_vm;
+            t->flags = (signed char)((t->flags & 31) | (cur_keep ? kFlagKeep : 0));
           }
           __syncwarp();
           const int rank = __popc(pm & lt_mask);
-          const int npush = min(__popc(pm), P.wdepth - sp);
+          const int npush = min(__popc(pm), D - sp);
           if (more) {
             Node *dst = nullptr;
             if (rank < npush) {
-              dst = wst + sp + rank;
+              dst = wst + wrap(wbot + sp + rank, D);
             } else {
               const unsigned long long k = atomicAdd(&ctl->nout, 1ull);
               if ((long long)k < P.out_cap) dst = P.out + k;
@@ -255,7 +270,6 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
           __syncwarp();
         }
         if (status == kStFork) {
-          // the fork's own state becomes its first child, in place
           if (first < 0) {
             set_entry(rcol, stride, fork_cell, fork_e & 0x7Fu, P.run_skip);
           } else {
@@ -283,41 +297,91 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
       }
     }
 
-    // ---- (B) refill idle lanes
+    // ---- (B) refill idle lanes: stack top, else the frontier input, else the pool
     for (;;) {
       const unsigned im = __ballot_sync(kFull, status == kStIdle);
       if (!im) break;
       if (!have_cur) {
         if (PERSIST && sp > 0) {
-          const Node *N = wst + sp - 1;
+          const Node *N = wst + wrap(wbot + sp - 1, D);
           cur_keep = (N->flags & kFlagKeep) ? 1 : 0;
           cur_vm = N->vmask;
           have_cur = true;
         } else {
-          if (input_done) break;
-          long long k = batch;
-          // once an epoch is ending, leave the rest of the input where it is
-          if (lane == 0 && !(PERSIST && *((volatile int *)&ctl->dump)))
-            k = (long long)atomicAdd(&ctl->cursor, 1ull);
-          k = __shfl_sync(kFull, k, 0);
-          if (k >= batch) {
-            input_done = true;
-            break;
+          const Node *src = nullptr;
+          bool from_pool = false;
+          if (!input_done) {
+            if (PERSIST && !busy) {
+              if (lane == 0) atomicAdd(&ctl->busy, 1);  // before any claim, so idle warps see work in flight
+              busy = true;
+            }
+            long long k = batch;
+            // once an epoch is ending, leave the rest of the input where it is
+            if (lane == 0 && !(PERSIST && *((volatile int *)&ctl->dump)))
+              k = (long long)atomicAdd(&ctl->cursor, 1ull);
+            k = __shfl_sync(kFull, k, 0);
+            if (k >= batch) input_done = true;
+            else src = P.stack + (top0 - 1 - k);
           }
-          const Node *src = P.stack + (top0 - 1 - k);
+          if (PERSIST && !src) {
+            long long h = -1;
+            int inc = 0;
+            if (lane == 0 && !*((volatile int *)&ctl->dump)) {
+              unsigned long long hh = *((volatile unsigned long long *)&ctl->pool_head);
+              const unsigned long long tl = *((volatile unsigned long long *)&ctl->pool_tail);
+              const unsigned long long lim = tl < (unsigned long long)P.pool_cap ? tl : (unsigned long long)P.pool_cap;
+              if (hh < lim && !busy) {
+                atomicAdd(&ctl->busy, 1);  // only when there is something to take
+                inc = 1;
+              }
+              while (hh < lim) {
+                const unsigned long long got = atomicCAS(&ctl->pool_head, hh, hh + 1);
+                if (got == hh) {
+                  h = (long long)hh;
+                  break;
+                }
+                hh = got;
+              }
+              if (h >= 0) {
+                // the donor claimed the slot before writing it; wait (bounded) for its data
+                const unsigned long long t0 = globaltimer();
+                while (*((volatile int *)&P.pool_ready[h]) != tag) {
+                  if (globaltimer() - t0 > 200000000ull) {
+                    atomicOr(&ctl->error, kErrTimeout);
+                    h = -1;
+                    break;
+                  }
+                  __nanosleep(64);
+                }
+                __threadfence();
+              }
+            }
+            h = __shfl_sync(kFull, h, 0);
+            if (__shfl_sync(kFull, inc, 0)) busy = true;
+            if (h >= 0) {
+              src = P.pool + h;
+              from_pool = true;
+            }
+          }
+          if (!src) break;
           if (PERSIST) {
-            copy_node(wst, src, lane);
+            wbot = 0;
+            if (from_pool) copy_node_cg(wst, src, lane);
+            else copy_node(wst, src, lane);
             __syncwarp();
             sp = 1;
+            cur_keep = (wst->flags & kFlagKeep) ? 1 : 0;
+            cur_vm = wst->vmask;
           } else {
             cur = src;
+            cur_keep = (src->flags & kFlagKeep) ? 1 : 0;
+            cur_vm = src->vmask;
           }
-          cur_keep = (src->flags & kFlagKeep) ? 1 : 0;
-          cur_vm = src->vmask;
           have_cur = true;
+          backoff = 256;
         }
       }
-      const Node *N = PERSIST ? (wst + sp - 1) : cur;
+      const Node *N = PERSIST ? (wst + wrap(wbot + sp - 1, D)) : cur;
       const int navail = cur_keep + __popcll(cur_vm);
       const int nidle = __popc(im);
       const int rank = __popc(im & lt_mask);
@@ -339,26 +403,37 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
 
     // ---- (C) end of work / end of epoch
     const bool any_run = __any_sync(kFull, status == kStRun);
-    if (!any_run && input_done && !have_cur && (!PERSIST || sp == 0)) {
-      if (PERSIST && lane == 0 && !counted_starve) atomicAdd(&ctl->starved, 1);
-      break;
-    }
-    if (PERSIST) {
+    const bool has_work = any_run || have_cur || (PERSIST && sp > 0);
+    if (!PERSIST) {
+      if (!has_work && input_done) break;
+    } else {
+      if (!has_work && busy) {
+        if (lane == 0) atomicSub(&ctl->busy, 1);
+        busy = false;
+      }
       int d = 0;
       if (lane == 0) {
         d = *((volatile int *)&ctl->dump);
         if (!d && globaltimer() - t_begin > (unsigned long long)P.epoch_ns) d = 1;
-        if (!d && *((volatile int *)&ctl->starved) >= P.starve_limit) d = 1;
         if (!d && (long long)*((volatile unsigned long long *)&ctl->nout) > P.out_soft) d = 1;
         if (d) *((volatile int *)&ctl->dump) = 1;
       }
       d = __shfl_sync(kFull, d, 0);
-      if (!d && input_done && sp == 0 && !have_cur && !counted_starve) {
-        const int nidle = __popc(__ballot_sync(kFull, status == kStIdle));
-        if (nidle >= 16) {
-          if (lane == 0) atomicAdd(&ctl->starved, 1);
-          counted_starve = true;
+      if (!has_work) {
+        // nothing here: done when no warp holds work and the pool is empty, else wait for a donation
+        int done = d;
+        if (lane == 0 && !done && input_done) {
+          const int b = *((volatile int *)&ctl->busy);
+          const unsigned long long hh = *((volatile unsigned long long *)&ctl->pool_head);
+          const unsigned long long tl = *((volatile unsigned long long *)&ctl->pool_tail);
+          const unsigned long long lim = tl < (unsigned long long)P.pool_cap ? tl : (unsigned long long)P.pool_cap;
+          done = (b == 0 && hh >= lim);
         }
+        done = __shfl_sync(kFull, done, 0);
+        if (done) break;
+        __nanosleep(backoff);
+        backoff = backoff < 8192 ? 2 * backoff : 8192;
+        continue;
       }
       if (d && rounds > 0) {
         // dump: live lanes as resume nodes, then this warp's stack
@@ -371,8 +446,9 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
           status = kStIdle;
         }
         if (have_cur && sp > 0 && lane == 0) {
-          wst[sp - 1].vmask = cur_vm;
-          wst[sp - 1].flags = (signed char)((wst[sp - 1].flags & 31) | (cur_keep ? kFlagKeep : 0));
+          Node *t = wst + wrap(wbot + sp - 1, D);
+          t->vmask = cur_vm;
+          t->flags = (signed char)((t->flags & 31) | (cur_keep ? kFlagKeep : 0));
         }
         __syncwarp();
         if (sp > 0) {
@@ -380,11 +456,31 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
           if (lane == 0) base = atomicAdd(&ctl->nout, (unsigned long long)sp);
           base = __shfl_sync(kFull, base, 0);
           for (int i = 0; i < sp; ++i) {
-            if ((long long)(base + i) < P.out_cap) copy_node(P.out + base + i, wst + i, lane);
+            if ((long long)(base + i) < P.out_cap) copy_node(P.out + base + i, wst + wrap(wbot + i, D), lane);
             else if (lane == 0) atomicOr(&ctl->error, kErrOutFull);
           }
         }
+        if (busy && lane == 0) atomicSub(&ctl->busy, 1);
         break;
+      }
+      // donate the oldest node of a deep stack when the pool runs low
+      if (sp >= 2) {
+        long long s = -1;
+        if (lane == 0) {
+          const unsigned long long hh = *((volatile unsigned long long *)&ctl->pool_head);
+          const unsigned long long tl = *((volatile unsigned long long *)&ctl->pool_tail);
+          if (tl < (unsigned long long)P.pool_cap && tl - hh < (unsigned long long)P.pool_low)
+            s = (long long)atomicAdd(&ctl->pool_tail, 1ull);
+        }
+        s = __shfl_sync(kFull, s, 0);
+        if (s >= 0 && s < P.pool_cap) {
+          copy_node(P.pool + s, wst + wbot, lane);
+          __threadfence();
+          __syncwarp();
+          if (lane == 0) atomicExch(&P.pool_ready[s], tag);
+          wbot = wrap(wbot + 1, D);
+          --sp;
+        }
       }
     }
 
@@ -459,25 +555,34 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
 }
 
 // Between launches: the input taken from the top of the stack is gone; the
-// outputs go where it was.
-__global__ void move_outputs(Ctl *ctl, Node *stack, const Node *out, long long cap) {
+// outputs, then the pool nodes nobody took, go where it was.
+__global__ void move_outputs(Ctl *ctl, Node *stack, const Node *out, const Node *pool, long long pool_cap,
+                             long long cap) {
   const long long used = min((long long)ctl->cursor, ctl->batch);
   const long long base = ctl->top - used;
   const long long n = (long long)ctl->nout;
-  if (base + n > cap || ctl->error) return;  // finish_launch reports the overflow
-  const long long chunks = n * kNodeChunks;
+  const long long ph = (long long)ctl->pool_head;
+  const long long pt = min((long long)ctl->pool_tail, pool_cap);
+  const long long np = pt > ph ? pt - ph : 0;
+  if (base + n + np > cap || ctl->error) return;  // finish_launch reports the overflow
+  const long long chunks = n * kNodeChunks, pchunks = np * kNodeChunks;
   uint4 *dst = reinterpret_cast<uint4 *>(stack + base);
   const uint4 *src = reinterpret_cast<const uint4 *>(out);
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < chunks; i += (long long)gridDim.x * blockDim.x)
-    dst[i] = src[i];
+  const uint4 *psrc = reinterpret_cast<const uint4 *>(pool + ph);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < chunks + pchunks;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = i < chunks ? src[i] : __ldcg(psrc + (i - chunks));
 }
 
-__global__ void finish_launch(Ctl *ctl, long long cap, long long batch_max) {
+__global__ void finish_launch(Ctl *ctl, long long cap, long long batch_max, long long pool_cap) {
   const long long used = min((long long)ctl->cursor, ctl->batch);
-  long long top = ctl->top - used + (long long)ctl->nout;
+  const long long ph = (long long)ctl->pool_head;
+  const long long pt = min((long long)ctl->pool_tail, pool_cap);
+  const long long np = pt > ph ? pt - ph : 0;
+  long long top = ctl->top - used + (long long)ctl->nout + np;
   if (top > cap || ctl->error) {
-    // the outputs did not fit: stop the search here and let the host report it
-    ctl->error |= kErrOverflow;
+    // the outputs did not fit (or a device wait ran out): stop here and let the host report it
+    if (top > cap) ctl->error |= kErrOverflow;
     top = 0;
   }
   ctl->top = top;
@@ -486,7 +591,9 @@ __global__ void finish_launch(Ctl *ctl, long long cap, long long batch_max) {
   ctl->cursor = 0;
   ctl->nout = 0;
   ctl->dump = 0;
-  ctl->starved = 0;
+  ctl->busy = 0;
+  ctl->pool_head = 0;
+  ctl->pool_tail = 0;
   ctl->launches += 1;
 }
 
@@ -557,6 +664,10 @@ struct e13_ctx {
   long long out_cap;
   Node *wstack;
   long long wstack_nodes;
+  Node *pool;
+  long long pool_cap;
+  int *pool_ready;
+  long long pool_ready_cap;
   SurvRec *surv;
   long long surv_cap;
   Ctl *ctl;
@@ -623,6 +734,8 @@ extern "C" void e13_ctx_destroy(e13_ctx *c) {
   cudaFree(c->stack);
   cudaFree(c->out);
   cudaFree(c->wstack);
+  cudaFree(c->pool);
+  cudaFree(c->pool_ready);
   cudaFree(c->surv);
   cudaFree(c->ctl);
   cudaFreeHost(c->ctl_host);
@@ -715,7 +828,7 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
     if (tuning->batch) tu.batch = tuning->batch;
     if (tuning->epoch_us) tu.epoch_us = tuning->epoch_us;
     if (tuning->epochs_per_graph) tu.epochs_per_graph = tuning->epochs_per_graph;
-    if (tuning->starve_pct) tu.starve_pct = tuning->starve_pct;
+    if (tuning->pool_low_pct) tu.pool_low_pct = tuning->pool_low_pct;
     tu.run_skip = tuning->run_skip;
     if (tuning->stack_nodes) tu.stack_nodes = tuning->stack_nodes;
   }
@@ -742,6 +855,8 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   if ((rc = grow(&c->stack, &c->stack_cap, stack_nodes))) return rc;
   if ((rc = grow(&c->out, &c->out_cap, out_nodes))) return rc;
   if (persist && (rc = grow(&c->wstack, &c->wstack_nodes, nwarps * tu.warp_stack))) return rc;
+  if (persist && (rc = grow(&c->pool, &c->pool_cap, kPoolNodes))) return rc;
+  if (persist && (rc = grow(&c->pool_ready, &c->pool_ready_cap, kPoolNodes))) return rc;
   const long long scap = std::max<long long>(surv_cap, 1024);
   if ((rc = grow(&c->surv, &c->surv_cap, scap))) return rc;
 
@@ -754,7 +869,10 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   P.run_skip = tu.run_skip ? 1 : 0;
   P.step_cap = tu.step_cap;
   P.wdepth = tu.warp_stack;
-  P.starve_limit = (int)std::max<long long>(1, nwarps * tu.starve_pct / 100);
+  P.pool_low = (int)std::max<long long>(1, nwarps * tu.pool_low_pct / 100);
+  P.pool_cap = c->pool_cap;
+  P.pool = c->pool;
+  P.pool_ready = c->pool_ready;
   P.out_cap = c->out_cap;
   P.out_soft = c->out_cap - dump_room - 1024;
   P.surv_cap = c->surv_cap;
@@ -777,6 +895,8 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   c->ctl_host->batch = 1;
   c->ctl_host->peak = 1;
   CK(cudaMemcpyAsync(c->stack, &root, sizeof root, cudaMemcpyHostToDevice, c->stream));
+  // pool slots carry the tag of the launch that wrote them; tags restart with every search
+  if (persist) CK(cudaMemsetAsync(c->pool_ready, 0, sizeof(int) * (size_t)c->pool_ready_cap, c->stream));
   CK(cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
   CK(cudaEventRecord(c->ev0, c->stream));
 
@@ -789,8 +909,8 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     for (int e = 0; e < tu.epochs_per_graph; ++e) {
       search_kernel<true><<<blocks, tu.block, smem, c->stream>>>(P);
-      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->stack_cap);
-      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, batch_max);
+      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, c->stack_cap);
+      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, batch_max, c->pool_cap);
     }
     CK(cudaStreamEndCapture(c->stream, &graph));
     CK(cudaGraphInstantiate(&exec, graph, 0));
@@ -801,7 +921,7 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
       CK(cudaMemcpyAsync(c->ctl_host, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
       CK(cudaStreamSynchronize(c->stream));
       if (c->ctl_host->error) {
-        err = (c->ctl_host->error & kErrOutFull) ? E13_ERR_OVERFLOW : E13_ERR_OVERFLOW;
+        err = (c->ctl_host->error & kErrTimeout) ? E13_ERR_TIMEOUT : E13_ERR_OVERFLOW;
         break;
       }
       if (c->ctl_host->top > c->stack_cap - (long long)out_nodes) {
@@ -815,8 +935,8 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   } else {
     for (;;) {
       search_kernel<false><<<blocks, tu.block, smem, c->stream>>>(P);
-      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->stack_cap);
-      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, batch_max);
+      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, c->stack_cap);
+      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, batch_max, c->pool_cap);
       launches += 3;
       search_launches += 1;
       CK(cudaGetLastError());

@@ -59,7 +59,7 @@ class Survivor(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int32), ("block", ctypes.c_int32), ("slice", ctypes.c_int32),
                 ("warp_stack", ctypes.c_int32), ("step_cap", ctypes.c_int32), ("batch", ctypes.c_int32),
-                ("epoch_us", ctypes.c_int32), ("epochs_per_graph", ctypes.c_int32), ("starve_pct", ctypes.c_int32),
+                ("epoch_us", ctypes.c_int32), ("epochs_per_graph", ctypes.c_int32), ("pool_low_pct", ctypes.c_int32),
                 ("run_skip", ctypes.c_int32), ("stack_nodes", ctypes.c_int64)]
 
 

@@ -77,7 +77,7 @@ typedef struct e13_survivor {
 /* Search kernels. */
 enum {
   E13_KERNEL_PLAIN = 0,      /* one launch per frontier batch, host sync per launch */
-  E13_KERNEL_PERSISTENT = 1  /* per-warp DFS epochs from a device work queue, graph-captured */
+  E13_KERNEL_PERSISTENT = 1  /* per-warp DFS with in-kernel work donation, graph-captured epochs */
 };
 
 /* Tunables of the device search (0 = library default; see e13_default_tuning). */
@@ -90,7 +90,7 @@ typedef struct e13_tuning {
   int32_t batch;             /* nodes taken from the frontier per launch / epoch (0 = auto) */
   int32_t epoch_us;          /* persistent: wall-clock bound of one epoch, microseconds */
   int32_t epochs_per_graph;  /* persistent: epochs captured in one CUDA graph */
-  int32_t starve_pct;        /* persistent: end an epoch when this % of warps starve */
+  int32_t pool_low_pct;      /* persistent: warps donate stack nodes while the pool holds fewer than this % of warps */
   int32_t run_skip;          /* 1: advance whole words across runs of a self-loop (exact) */
   int64_t stack_nodes;       /* frontier stack capacity in nodes (0 = auto) */
 } e13_tuning;

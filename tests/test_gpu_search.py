@@ -106,7 +106,7 @@ def test_symmetric_vs_oracle():
 
 
 @pytest.mark.parametrize("tune", [dict(slice=1), dict(slice=7, warp_stack=1), dict(block=256, slice=64),
-                                  dict(warp_stack=3, starve_pct=1, epoch_us=200),
+                                  dict(warp_stack=3, pool_low_pct=1, epoch_us=200), dict(warp_stack=2, pool_low_pct=100, epoch_us=50),
                                   dict(kernel=E.KERNEL_PLAIN, step_cap=50, batch=3)])
 def test_tunings_do_not_change_results(searches, tune):
     e = searches["local_edits_f2"]
