@@ -748,6 +748,13 @@ extern "C" void e13_ctx_destroy(e13_ctx *c) {
 }
 
 extern "C" int e13_ctx_device(const e13_ctx *c) { return c ? c->device : 0; }
+extern "C" cudaStream_t e13_ctx_stream(const e13_ctx *c) { return c->stream; }
+extern "C" void e13_ctx_note_run(e13_ctx *c, double ms, long long launches) {
+  memset(&c->stats, 0, sizeof c->stats);
+  c->stats.device_ms = ms;
+  c->stats.launches = launches;
+  c->stats.search_kernel_launches = launches;
+}
 
 extern "C" int e13_last_stats(const e13_ctx *c, e13_stats *out) {
   if (!c || !out) return E13_ERR_ARG;

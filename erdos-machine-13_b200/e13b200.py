@@ -123,6 +123,8 @@ def lib():
         L.e13_last_stats.argtypes = [ctypes.c_void_p, P(Stats)]
         L.e13_run_full.argtypes = [ctypes.c_void_p, P(ctypes.c_int32), I, I, P(ctypes.c_int64)]
         L.e13_check.argtypes = [ctypes.c_void_p, P(CheckIn), I, I, I, P(CheckOut)]
+        L.e13_raw_run.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int64, I,
+                                  ctypes.c_int64, P(ctypes.c_int64), P(ctypes.c_uint64)]
         L.e13_parse_survivor_line.argtypes = [ctypes.c_char_p, P(CheckIn)]
         L.e13_format_recheck.argtypes = [P(CheckOut), I, ctypes.c_char_p, ctypes.c_size_t]
         L.e13_format_deep.argtypes = [P(CheckIn), P(CheckOut), I, ctypes.c_char_p, ctypes.c_size_t]
@@ -133,7 +135,7 @@ def lib():
 EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine", "e13_setup",
             "e13_format_survivor", "e13_format_summary", "e13_default_tuning", "e13_ctx_create", "e13_ctx_destroy",
             "e13_search", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
-            "e13_format_recheck", "e13_format_deep"]
+            "e13_format_recheck", "e13_format_deep", "e13_raw_run"]
 
 
 def keys():
@@ -230,6 +232,16 @@ class Context:
         if r:
             raise E13Error(r, "e13_run_full")
         return [list(out[7 * i: 7 * i + 7]) for i in range(n)]
+
+    def raw_run(self, n, nq=13, max_steps=1 << 18, seed=0, codes: bytes | None = None, want_out=True):
+        """Raw-simulator set; returns (per-machine [steps, status, head, ones] or None, total steps)."""
+        out = (ctypes.c_int64 * (4 * n))() if want_out else None
+        tot = ctypes.c_uint64()
+        r = lib().e13_raw_run(self.h, codes, seed, n, nq, max_steps, out, ctypes.byref(tot))
+        if r:
+            raise E13Error(r, "e13_raw_run")
+        rows = [list(out[4 * i: 4 * i + 4]) for i in range(n)] if want_out else None
+        return rows, tot.value
 
     def check(self, ins, nmax, mode=0):
         n = len(ins)

@@ -165,6 +165,19 @@ int e13_last_stats(const e13_ctx *ctx, e13_stats *out);
    {survived, stage, st0, head0, abs, rel, steps} as 7 int64. */
 int e13_run_full(e13_ctx *ctx, const int32_t *tabs, int n, int nq, int64_t *out);
 
+/* Raw-simulator throughput set: n whole tables run from the blank tape with
+   no filter, at most max_steps steps each, stopping when the head leaves the
+   window -64..1299 or reads a halt -- steps (3)-(7) of run()
+   (src/e13search.c:163-175) without the stage test and the deadline; the step
+   that leaves the window is not counted, as in run().  codes: n * 2*nq bytes
+   (0..4nq-1 = moves, anything else = halt), or NULL to draw them on the device:
+   cell i of machine m = splitmix64 draw m*2nq+i+1 from `seed`, mod 4nq (each
+   cell uniform over write x dir x next).  out (may be NULL): per machine
+   {steps, status (0 step cap, 1 left the window, 2 halt), final head, ones}.
+   *total_steps (may be NULL) = sum of steps.  Device time: e13_last_stats. */
+int e13_raw_run(e13_ctx *ctx, const uint8_t *codes, uint64_t seed, int64_t n, int nq, int64_t max_steps,
+                int64_t *out, uint64_t *total_steps);
+
 /* ---- hash-free deep checker (src/recheck.c, src/deep.c) ---- */
 
 enum { E13_CHECK_RECHECK = 0, E13_CHECK_DEEP = 1 };

@@ -636,3 +636,55 @@ int oracle_deep_line(const char *line, int nmax, char *out, int olen) {
   free(tape);
   return failed ? 0 : 1;
 }
+
+/* ------------------------------------------------------------------ */
+/* raw simulator (no filter)                                           */
+
+/* Draw k (1-based) of splitmix64 from `seed`: the generator's state after k
+   increments is seed + k * golden, so any draw can be made directly. */
+static uint64_t mix_draw(uint64_t seed, uint64_t k) {
+  uint64_t s = seed + (k - 1) * 0x9E3779B97F4A7C15ULL;
+  return mix_next(&s);
+}
+
+/* Random tables: machine m, cell i = draw m*2nq + i + 1 mod 4nq, i.e. each
+   cell uniform over write x dir x next (no halt).  codes: n * 2nq bytes. */
+void oracle_raw_tables(uint64_t seed, long n, int nq, unsigned char *codes) {
+  for (long m = 0; m < n; m++)
+    for (int i = 0; i < 2 * nq; i++)
+      codes[m * 2 * nq + i] = (unsigned char)(mix_draw(seed, (uint64_t)(m * 2 * nq + i + 1)) % (uint64_t)(4 * nq));
+}
+
+/* Steps (3)-(7) of run() (src/e13search.c:163-175) with the stage test and
+   the deadline removed: a table runs from the blank tape for at most
+   max_steps steps and stops when the head leaves the window (head <= -64 or
+   >= 1299; that step is not counted, as in run()) or reads a halt.  out (4 per
+   machine): steps, status (0 step cap, 1 left the window, 2 halt), final
+   head, ones on the tape. */
+void oracle_raw_run(const unsigned char *codes, long n, int nq, long max_steps, long long *out) {
+  unsigned char tape[O_TAPE];
+  for (long m = 0; m < n; m++) {
+    const unsigned char *tab = codes + m * 2 * nq;
+    memset(tape, 0, sizeof tape);
+    int head = 0, st = 0, status = 0;
+    long t = 0;
+    long long ones = 0;
+    while (t < max_steps) {
+      int p = head + O_LEFT, sym = tape[p];
+      int code = tab[2 * st + sym];
+      if (code >= 4 * nq) { status = 2; break; }
+      if ((code & 1) != sym) {
+        tape[p] = (unsigned char)(code & 1);
+        ones += (code & 1) ? 1 : -1;
+      }
+      head += (code & 2) ? 1 : -1;
+      if (head <= -O_LEFT || head >= O_RIGHT - 1) { status = 1; break; }
+      st = code >> 2;
+      t++;
+    }
+    out[4 * m] = t;
+    out[4 * m + 1] = status;
+    out[4 * m + 2] = head;
+    out[4 * m + 3] = ones;
+  }
+}

@@ -42,6 +42,8 @@ def lib():
         L.oracle_run_full.argtypes = [P(I), I, P(ctypes.c_longlong)]
         L.oracle_recheck_line.argtypes = [ctypes.c_char_p, I, ctypes.c_char_p, I, ctypes.c_char_p, I]
         L.oracle_deep_line.argtypes = [ctypes.c_char_p, I, ctypes.c_char_p, I]
+        L.oracle_raw_tables.argtypes = [ctypes.c_uint64, ctypes.c_long, I, ctypes.c_char_p]
+        L.oracle_raw_run.argtypes = [ctypes.c_char_p, ctypes.c_long, I, ctypes.c_long, P(ctypes.c_longlong)]
         _lib = L
     return _lib
 
@@ -174,3 +176,16 @@ def parse_summary(line: str):
         return None
     return dict(X=int(m.group(1)), leaves=int(m.group(2)), survivors=int(m.group(3)),
                 steps=int(m.group(4)) if m.group(4) else None, hist=[int(x) for x in m.group(5).split()])
+
+
+def raw_tables(seed: int, n: int, nq: int = 13) -> bytes:
+    """Random tables of the raw-simulator set (splitmix64 draws, mod 4nq)."""
+    buf = ctypes.create_string_buffer(n * 2 * nq)
+    lib().oracle_raw_tables(seed, n, nq, buf)
+    return buf.raw
+
+
+def raw_run(codes: bytes, n: int, nq: int = 13, max_steps: int = 1 << 18):
+    out = (ctypes.c_longlong * (4 * n))()
+    lib().oracle_raw_run(codes, n, nq, max_steps, out)
+    return [list(out[4 * i: 4 * i + 4]) for i in range(n)]

@@ -152,3 +152,26 @@ def test_run_skip_is_exact(searches, name):
     b = run_entry(e, E.tuning(run_skip=1))
     assert a == b
     check_entry(e, b[0])
+
+
+def test_raw_simulator_vs_oracle():
+    """Raw-simulator set (no filter, <= 2^18 steps, stop off the window): the
+    device, drawing its own tables from seed 0, equals the oracle on the first
+    3000 machines, and on tables passed in from the host."""
+    n = 3000
+    codes = O.raw_tables(0, n)
+    exp = O.raw_run(codes, n)
+    got, tot = ctx().raw_run(n, seed=0)
+    assert got == exp and tot == sum(r[0] for r in exp)
+    got2, _ = ctx().raw_run(n, codes=codes)
+    assert got2 == exp
+
+
+def test_run_full_matches_oracle_random_tables():
+    """Whole-table runs (with the filter) of random 13-state tables against
+    the oracle."""
+    codes = O.raw_tables(7, 2000)
+    tabs = [list(codes[26 * i: 26 * i + 26]) for i in range(2000)]
+    got = ctx().run_full(tabs, 13)
+    for t, g in zip(tabs, got):
+        assert g == O.run_full(t, 13)

@@ -163,3 +163,26 @@ def test_oracle_vs_reference_binary(args):
         check_counts(c, ref[0])
         got_surv = [O.survivor_line(X, rr, job.nq) for rr in recs]
     assert sorted(got_surv) == ref_surv
+
+
+def test_raw_tables_are_splitmix_draws():
+    """Machine m, cell i = draw m*26+i+1 of splitmix64 from seed 0, mod 52."""
+    M = (1 << 64) - 1
+    s = 0
+    exp = []
+    for _ in range(3 * 26):
+        s = (s + 0x9E3779B97F4A7C15) & M
+        z = s
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+        exp.append((z ^ (z >> 31)) % 52)
+    assert list(O.raw_tables(0, 3)) == exp
+
+
+def test_raw_run_small_known_cases():
+    # A0 = 1RA: writes ones rightwards; leaves the window at 1299 (that step not counted)
+    codes = bytes([2 | 1, 2 | 1]) + bytes([0] * 24)
+    assert O.raw_run(codes, 1, nq=13)[0] == [1298, 1, 1299, 1299]
+    # A0 = 0LA: walks left over blanks, leaves at -64 after 63 counted steps
+    codes = bytes([0, 0]) + bytes([0] * 24)
+    assert O.raw_run(codes, 1, nq=13)[0] == [63, 1, -64, 0]
