@@ -10,6 +10,7 @@
 // step: stage test, deadline, read, fork on a first read, halt, write + hash,
 // move, window bounds, state, t++.
 #pragma once
+#include <stddef.h>
 #include <stdint.h>
 
 namespace e13dev {
@@ -47,12 +48,15 @@ struct __align__(16) Node {
   signed char nt, stage, st0, flags;
   short p0, pend;
   unsigned char nintro, budget, pad0, pad1;
-  u32 pad2;
+  u32 pad2[3];
   unsigned short cellv[32];  // cell entries with the self-loop bit; row s = cellv[2s] | cellv[2s+1] << 16
   u32 tape[kTapeWords];
-  u32 pad3[5];
+  u32 pad3;
 };
 static_assert(sizeof(Node) % 16 == 0, "Node must be a whole number of 16-byte chunks");
+// cellv is read and written as uint4 (four rows at a time): it must start on a 16-byte boundary
+static_assert(offsetof(Node, cellv) % 16 == 0, "Node::cellv must be 16-byte aligned");
+static_assert(offsetof(Node, tape) % 4 == 0, "Node::tape must be word aligned");
 constexpr int kNodeChunks = sizeof(Node) / 16;
 
 // Survivor record written by the device.
