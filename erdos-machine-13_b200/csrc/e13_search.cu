@@ -1012,3 +1012,54 @@ extern "C" int e13_run_full(e13_ctx *c, const int32_t *tabs, int n, int nq, int6
   cudaFree(d_out);
   return E13_OK;
 }
+
+// ------------------------------------------------------------------------
+// autotuner
+
+extern "C" int e13_autotune(e13_ctx *c, const e13_job *job, const e13_tuning *start, e13_tuning *best,
+                            double *best_ms) {
+  if (!c || !job || !best) return E13_ERR_ARG;
+  e13_tuning cur;
+  if (start) cur = *start;
+  else e13_default_tuning(&cur);
+  cur.kernel = E13_KERNEL_PERSISTENT;
+  e13_counts ref_counts, got;
+  int ns = 0;
+  std::vector<e13_survivor> surv(4096);
+  // every candidate must give the same totals: a free determinism check
+  int rc = e13_search(c, job, &cur, &ref_counts, surv.data(), (int)surv.size(), &ns);
+  if (rc && rc != E13_ERR_SURV_CAP) return rc;
+  double cur_ms = c->stats.device_ms;
+  struct Axis {
+    int32_t e13_tuning::*field;
+    int vals[4];
+    int n;
+  };
+  const Axis axes[] = {
+      {&e13_tuning::block, {512, 640, 768, 0}, 3},
+      {&e13_tuning::slice, {16, 32, 64, 128}, 4},
+      {&e13_tuning::warp_stack, {16, 32, 64, 128}, 4},
+      {&e13_tuning::pool_low_pct, {5, 12, 25, 50}, 4},
+  };
+  for (const Axis &ax : axes) {
+    e13_tuning axis_best = cur;
+    double axis_ms = cur_ms;
+    for (int i = 0; i < ax.n; ++i) {
+      if (ax.vals[i] == cur.*(ax.field)) continue;
+      e13_tuning t = cur;
+      t.*(ax.field) = ax.vals[i];
+      rc = e13_search(c, job, &t, &got, surv.data(), (int)surv.size(), &ns);
+      if (rc && rc != E13_ERR_SURV_CAP) return rc;
+      if (memcmp(&got, &ref_counts, sizeof got) != 0) return E13_ERR_CUDA;  // results must not depend on tuning
+      if (c->stats.device_ms < axis_ms) {
+        axis_ms = c->stats.device_ms;
+        axis_best = t;
+      }
+    }
+    cur = axis_best;
+    cur_ms = axis_ms;
+  }
+  *best = cur;
+  if (best_ms) *best_ms = cur_ms;
+  return E13_OK;
+}

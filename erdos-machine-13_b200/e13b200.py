@@ -121,6 +121,7 @@ def lib():
         L.e13_ctx_destroy.restype = None
         L.e13_search.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Counts), P(Survivor), I, P(I)]
         L.e13_last_stats.argtypes = [ctypes.c_void_p, P(Stats)]
+        L.e13_autotune.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Tuning), P(ctypes.c_double)]
         L.e13_run_full.argtypes = [ctypes.c_void_p, P(ctypes.c_int32), I, I, P(ctypes.c_int64)]
         L.e13_check.argtypes = [ctypes.c_void_p, P(CheckIn), I, I, I, P(CheckOut)]
         L.e13_raw_run.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int64, I,
@@ -135,7 +136,7 @@ def lib():
 EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine", "e13_setup",
             "e13_format_survivor", "e13_format_summary", "e13_default_tuning", "e13_ctx_create", "e13_ctx_destroy",
             "e13_search", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
-            "e13_format_recheck", "e13_format_deep", "e13_raw_run"]
+            "e13_format_recheck", "e13_format_deep", "e13_raw_run", "e13_autotune"]
 
 
 def keys():
@@ -215,6 +216,16 @@ class Context:
         if r and r != -7:
             raise E13Error(r, "e13_search")
         return counts, [surv[i] for i in range(min(ns.value, surv_cap))]
+
+    def autotune(self, job: Job, start: Tuning | None = None):
+        """Coordinate-descent tuning of the persistent kernel on `job`; returns (Tuning, best ms)."""
+        best = Tuning()
+        ms = ctypes.c_double()
+        r = lib().e13_autotune(self.h, ctypes.byref(job), ctypes.byref(start) if start else None, ctypes.byref(best),
+                               ctypes.byref(ms))
+        if r:
+            raise E13Error(r, "e13_autotune")
+        return best, ms.value
 
     def stats(self) -> Stats:
         s = Stats()

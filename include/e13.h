@@ -156,6 +156,16 @@ void e13_ctx_destroy(e13_ctx *ctx);
 int e13_search(e13_ctx *ctx, const e13_job *job, const e13_tuning *tuning, e13_counts *counts,
                e13_survivor *surv, int surv_cap, int *nsurv);
 
+/* Autotuner (no counterpart in the reference, which has one fixed GPU
+   launch shape): coordinate descent over block size (lanes per CTA), slice
+   (steps between refills), warp_stack (subtree depth kept private to a warp
+   before it spills to the frontier) and pool_low_pct (donation threshold),
+   timing the persistent kernel on `job` with CUDA events.  Use a job that runs
+   in well under a second as the proxy for a larger one.  Every candidate must
+   reproduce the same counts, else E13_ERR_CUDA.  start may be NULL
+   (defaults); *best_ms (may be NULL) is the best device time. */
+int e13_autotune(e13_ctx *ctx, const e13_job *job, const e13_tuning *start, e13_tuning *best, double *best_ms);
+
 /* Statistics of the last e13_search on this context. */
 int e13_last_stats(const e13_ctx *ctx, e13_stats *out);
 

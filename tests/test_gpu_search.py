@@ -175,3 +175,14 @@ def test_run_full_matches_oracle_random_tables():
     got = ctx().run_full(tabs, 13)
     for t, g in zip(tabs, got):
         assert g == O.run_full(t, 13)
+
+
+def test_autotune_keeps_results(searches):
+    """The autotuner times candidate launch shapes on a proxy job; every
+    candidate must reproduce the same counts, and the tuning it returns too."""
+    e = searches["local_edits_f3"]
+    job = __import__("gpu_common").make_job(e, 12)
+    best, ms = ctx().autotune(job)
+    assert ms > 0 and best.block in (512, 640, 768)
+    c, _ = ctx().search(job, best)
+    assert c.as_dict()["leaves"] == e["expect"][12]["leaves"]
