@@ -217,6 +217,8 @@ def main():
     ctx = E.Context(local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
+    kstats = dict(lane_rounds=0.0, warp_rounds=0, donations=0, pool_claims=0, idle_polls=0, epochs=0)
+
     def one_step():
         steps = leaves = 0
         dev_ms = 0.0
@@ -230,6 +232,12 @@ def main():
             dev_ms += st.device_ms
             launches += st.launches
             surv_bytes += 64 * len(surv)
+            kstats["lane_rounds"] += st.lane_occupancy * st.warp_rounds
+            kstats["warp_rounds"] += st.warp_rounds
+            kstats["donations"] += st.donations
+            kstats["pool_claims"] += st.pool_claims
+            kstats["idle_polls"] += st.idle_polls
+            kstats["epochs"] += st.epochs
         return steps, leaves, dev_ms, launches, surv_bytes
 
     for _ in range(args.warmup):
@@ -283,7 +291,11 @@ def main():
             "e2e": {"value": tot["steps"] / tot["wall"], "unit": "steps/s",
                     "h2d_bytes_per_step": 288 * len(jobs) + 160 * len(jobs),
                     "d2h_bytes_per_step": tot["d2h"] // args.steps + 160 * len(jobs)},
-            "gpu_launches": tot["launches"], "clocks": clocks}
+            "gpu_launches": tot["launches"], "clocks": clocks,
+            "kernel_stats": {"lane_occupancy": kstats["lane_rounds"] / max(kstats["warp_rounds"], 1),
+                             "warp_rounds": kstats["warp_rounds"], "donations": kstats["donations"],
+                             "pool_claims": kstats["pool_claims"], "idle_polls": kstats["idle_polls"],
+                             "epochs": kstats["epochs"], "note": "all warmup and timed steps"}}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         s, l, dt, kind = run_reference_cpu(WORKLOADS[CPU_SAMPLE], threads)

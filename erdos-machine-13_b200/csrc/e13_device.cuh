@@ -79,6 +79,9 @@ struct Ctl {
   int launches;
   u64 leaves, steps;
   u64 hist[kStages + 1];
+  // utilisation counters: warp rounds, running lanes summed over rounds,
+  // pool donations and claims, idle-warp polls
+  u64 rounds, lane_rounds, donations, claims, polls;
   // persistent: nodes donated by warps with deep stacks to warps without work
   // (slots [pool_head, pool_tail) are waiting; each counter on its own cache line)
   alignas(128) unsigned long long pool_head;

@@ -217,6 +217,8 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   bool busy = false;           // persistent: counted in ctl->busy
   int rounds = 0;              // slices run: a warp dumps only after one (progress every epoch)
   unsigned backoff = 256;
+  unsigned long long st_lane_rounds = 0, st_polls = 0;
+  unsigned st_donations = 0, st_claims = 0;
 
   for (;;) {
     // ---- (A) forks
@@ -361,6 +363,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
             if (h >= 0) {
               src = P.pool + h;
               from_pool = true;
+              ++st_claims;
             }
           }
           if (!src) break;
@@ -431,6 +434,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
         }
         done = __shfl_sync(kFull, done, 0);
         if (done) break;
+        ++st_polls;
         __nanosleep(backoff);
         backoff = backoff < 8192 ? 2 * backoff : 8192;
         continue;
@@ -480,12 +484,14 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
           if (lane == 0) atomicExch(&P.pool_ready[s], tag);
           wbot = wrap(wbot + 1, D);
           --sp;
+          ++st_donations;
         }
       }
     }
 
     // ---- (D) run a slice
     ++rounds;
+    st_lane_rounds += __popc(__ballot_sync(kFull, status == kStRun));
     if (status == kStRun) {
       int n = P.slice;
       for (;;) {
@@ -545,6 +551,11 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   if (lane == 0) {
     atomicAdd(&s_leaves, wl);
     atomicAdd(&s_steps, ws);
+    atomicAdd(&ctl->rounds, (unsigned long long)rounds);
+    atomicAdd(&ctl->lane_rounds, st_lane_rounds);
+    atomicAdd(&ctl->polls, st_polls);
+    if (st_donations) atomicAdd(&ctl->donations, (unsigned long long)st_donations);
+    if (st_claims) atomicAdd(&ctl->claims, (unsigned long long)st_claims);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -624,7 +635,7 @@ __global__ void __launch_bounds__(256) run_full_kernel(const int *tabs, int n, i
   }
   Lane L;
   L.p = kLeft; L.st = 0; L.t = 0; L.deadline = c_deadline[1]; L.hb = 0; L.tgt = c_tgt[1];
-  L.nt = 1; L.stage = 0; L.st0 = -1; L.p0 = 0; L.flags = 3; L.ch0 = L.ch1 = L.ch2 = 0;
+  L.nt = 1; L.stage = 0; L.st0 = -1; L.p0 = kLeft; L.flags = 3; L.ch0 = L.ch1 = L.ch2 = 0;  // head0 = 0 until stage 1
   int ev;
   for (;;) {
     int nn = 1 << 30, cell = 0;
@@ -779,6 +790,7 @@ static void build_root(const e13_job *job, Node *root) {
   root->deadline = 4 * 2 + 64;
   root->nt = 1;
   root->st0 = -1;
+  root->p0 = kLeft;  // head0 = 0 until stage 1 sets it (src/e13search.c:123-129)
   root->flags = (signed char)(kFlagAbs | kFlagRel | kFlagKeep);
   root->pend = -1;
   root->nintro = (unsigned char)(job->sym_n0 < 0 ? 0 : job->sym_n0);
@@ -970,6 +982,12 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   c->stats.search_kernel_launches = search_launches;
   c->stats.epochs = c->ctl_host->launches;
   c->stats.peak_nodes = c->ctl_host->peak;
+  c->stats.lane_occupancy =
+      c->ctl_host->rounds ? (double)c->ctl_host->lane_rounds / (32.0 * (double)c->ctl_host->rounds) : 0.0;
+  c->stats.warp_rounds = (int64_t)c->ctl_host->rounds;
+  c->stats.donations = (int64_t)c->ctl_host->donations;
+  c->stats.pool_claims = (int64_t)c->ctl_host->claims;
+  c->stats.idle_polls = (int64_t)c->ctl_host->polls;
   if (err) return err;
 
   const Ctl &h = *c->ctl_host;

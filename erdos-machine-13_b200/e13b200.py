@@ -66,7 +66,9 @@ class Tuning(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("device_ms", ctypes.c_double), ("launches", ctypes.c_int64), ("epochs", ctypes.c_int64),
                 ("peak_nodes", ctypes.c_int64), ("search_kernel_launches", ctypes.c_int64),
-                ("search_kernel_ms", ctypes.c_double)]
+                ("search_kernel_ms", ctypes.c_double), ("lane_occupancy", ctypes.c_double),
+                ("warp_rounds", ctypes.c_int64), ("donations", ctypes.c_int64), ("pool_claims", ctypes.c_int64),
+                ("idle_polls", ctypes.c_int64)]
 
 
 E13_CHECK_MAX_NMAX = 20

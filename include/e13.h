@@ -103,6 +103,11 @@ typedef struct e13_stats {
   int64_t peak_nodes;        /* peak frontier stack */
   int64_t search_kernel_launches;
   double search_kernel_ms;   /* CUDA-event time summed over the search kernel's launches */
+  double lane_occupancy;     /* running lanes / 32 averaged over warp rounds */
+  int64_t warp_rounds;       /* warp rounds (slice + refill) */
+  int64_t donations;         /* persistent: stack nodes donated to the pool */
+  int64_t pool_claims;       /* persistent: pool nodes taken by warps without work */
+  int64_t idle_polls;        /* persistent: polls by warps waiting for work */
 } e13_stats;
 
 typedef struct e13_ctx e13_ctx;
