@@ -202,6 +202,60 @@ __device__ __forceinline__ int step_slice(int &p, int &st, int &t, const int dea
   return kEvRun;
 }
 
+// One action of a running lane, the unit of the warp's lock-step loop: one
+// step, one run skip, one stage test or one first-read event.  Every running
+// lane of a warp takes exactly one action per iteration, so the warp stays
+// converged except inside the rare branches, which rejoin at the end of the
+// iteration.  Returns 0 (go on), kEvDead, kEvSurv or kEvCell (a cell whose
+// entry has kEntSpecial; *cell and *ecell say which).  Same semantics as
+// step_slice(): each step follows src/e13search.c:134-177 in order.
+__device__ __forceinline__ int stage_check(struct Lane &L, const u32 *tcol, const u64 *keyc, int stride);
+
+__device__ __forceinline__ int lane_act(Lane &L, u32 *__restrict__ tcol, const u32 *__restrict__ rcol,
+                                        const u64 *__restrict__ keyb, const u64 *__restrict__ keyc, const int stride,
+                                        int &cell, u32 &ecell) {
+  if (L.t > L.deadline) return kEvDead;
+  const int p = L.p;
+  const int widx = (p >> 5) * stride;
+  const u32 word = tcol[widx];
+  const u32 row = rcol[L.st * stride];
+  const u32 sym = (word >> (p & 31)) & 1u;
+  const u32 e = (row >> (sym << 4)) & 0x1FFu;
+  if (e & (kEntSpecial | kEntSelf)) {
+    if (e & kEntSpecial) {
+      cell = (L.st << 1) | (int)sym;
+      ecell = e & 0xFFu;
+      return kEvCell;
+    }
+    if (L.hb != L.tgt) {
+      // run skip (see step_slice): exact while hb, the state and the ones stay put
+      const bool right = (e & 2u) != 0;
+      int lim = L.deadline - L.t + 1;
+      const int room = right ? (kTapeCells - 2) - p : p - 1;
+      lim = lim < room ? lim : room;
+      if (lim > 1) {
+        const int k = run_length(tcol, stride, p, sym, right, lim);
+        if (k > 1) {
+          L.p = p + (right ? k : -k);
+          L.t += k;
+          return 0;
+        }
+      }
+    }
+  }
+  if ((e ^ sym) & 1u) {
+    tcol[widx] = word ^ (1u << (p & 31));
+    L.hb ^= keyb[p];  // zero for cells < -2: those go to the counter hash
+  }
+  const int np = p + (int)(e & 2u) - 1;
+  if ((unsigned)(np - 1) >= (unsigned)(kTapeCells - 2)) return kEvDead;  // head <= -64 or >= 1299
+  L.p = np;
+  L.st = (int)((e >> 2) & 15u);
+  ++L.t;
+  if (L.hb == L.tgt) return stage_check(L, tcol, keyc, stride);
+  return 0;
+}
+
 // Counter hash from the tape: XOR of the keys of the ones at cells < -2
 // (exactly what the reference accumulates in hc, src/e13search.c:170).
 __device__ __forceinline__ u64 counter_hash(const u32 *tcol, const u64 *keyc, int stride) {

@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
             if (k >= batch) input_done = true;
             else src = P.stack + (top0 - 1 - k);
           }
-          if (PERSIST && !src) {
+          if (PERSIST && !src && (im == kFull || (rounds & 3) == 0)) {
             long long h = -1;
             int inc = 0;
             if (lane == 0 && !*((volatile int *)&ctl->dump)) {
@@ -415,13 +415,15 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
         busy = false;
       }
       int d = 0;
-      if (lane == 0) {
-        d = *((volatile int *)&ctl->dump);
-        if (!d && globaltimer() - t_begin > (unsigned long long)P.epoch_ns) d = 1;
-        if (!d && (long long)*((volatile unsigned long long *)&ctl->nout) > P.out_soft) d = 1;
-        if (d) *((volatile int *)&ctl->dump) = 1;
+      if (!has_work || (rounds & 7) == 0) {  // the control words are in L2: read them every 8th round
+        if (lane == 0) {
+          d = *((volatile int *)&ctl->dump);
+          if (!d && globaltimer() - t_begin > (unsigned long long)P.epoch_ns) d = 1;
+          if (!d && (long long)*((volatile unsigned long long *)&ctl->nout) > P.out_soft) d = 1;
+          if (d) *((volatile int *)&ctl->dump) = 1;
+        }
+        d = __shfl_sync(kFull, d, 0);
       }
-      d = __shfl_sync(kFull, d, 0);
       if (!has_work) {
         // nothing here: done when no warp holds work and the pool is empty, else wait for a donation
         int done = d;
@@ -468,7 +470,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
         break;
       }
       // donate the oldest node of a deep stack when the pool runs low
-      if (sp >= 2) {
+      if (sp >= 2 && (rounds & 3) == 0) {
         long long s = -1;
         if (lane == 0) {
           const unsigned long long hh = *((volatile unsigned long long *)&ctl->pool_head);
@@ -489,55 +491,51 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
       }
     }
 
-    // ---- (D) run a slice
+    // ---- (D) run a slice: every running lane takes one action per iteration
     ++rounds;
-    st_lane_rounds += __popc(__ballot_sync(kFull, status == kStRun));
-    if (status == kStRun) {
-      int n = P.slice;
-      for (;;) {
-        int cell = 0;
-        int ev = step_slice(L.p, L.st, L.t, L.deadline, L.hb, L.tgt, tcol, rcol, keyb, stride, n, cell);
-        if (ev == kEvRun) break;
-        if (ev == kEvStage) {
-          ev = stage_check(L, tcol, keyc, stride);
-          if (ev == 0) {
-            if (n > 0) continue;
-            break;
-          }
-        } else if (ev == kEvCell) {
-          const u32 e = get_entry(rcol, stride, cell);
-          if (e == kEntHalt) {
-            ev = kEvDead;
-          } else if (e == kEntFree || L.budget > 0) {
-            steps += (unsigned long long)(L.t - L.tseg);
-            L.tseg = L.t;
-            fork_cell = cell;
-            fork_e = e;
-            status = kStFork;
-            break;
-          } else {
-            // first read with nothing to branch on: the cell is now fixed
-            set_entry(rcol, stride, cell, e & 0x7Fu, P.run_skip);
-            if ((e & 0x7Fu) == kEntHalt) ev = kEvDead;
-            else continue;
+    {
+      const unsigned rm = __ballot_sync(kFull, status == kStRun);
+      st_lane_rounds += __popc(rm);
+      if (rm) {
+#pragma unroll 1
+        for (int it = 0; it < P.slice; ++it) {
+          if (status == kStRun) {
+            int cell = 0;
+            u32 e = 0;
+            int ev = lane_act(L, tcol, rcol, keyb, keyc, stride, cell, e);
+            if (ev == kEvCell) {
+              if (e == kEntHalt) {
+                ev = kEvDead;
+              } else if (e == kEntFree || L.budget > 0) {
+                // a fork: handled by the warp at the next round
+                steps += (unsigned long long)(L.t - L.tseg);
+                L.tseg = L.t;
+                fork_cell = cell;
+                fork_e = e;
+                status = kStFork;
+                ev = 0;
+              } else {
+                // first read with nothing to branch on: the cell is now fixed
+                set_entry(rcol, stride, cell, e & 0x7Fu, P.run_skip);
+                ev = ((e & 0x7Fu) == kEntHalt) ? kEvDead : 0;
+              }
+            }
+            if (ev) {
+              // a leaf
+              steps += (unsigned long long)(L.t - L.tseg);
+              L.tseg = L.t;
+              ++leaves;
+              if (ev == kEvDead) atomicAdd(&s_hist[L.stage], 1ull);
+              else record_survivor(P, L, rcol, stride);
+              status = kStIdle;
+            }
           }
         }
-        // a leaf
-        steps += (unsigned long long)(L.t - L.tseg);
-        L.tseg = L.t;
-        ++leaves;
-        if (ev == kEvDead) {
-          atomicAdd(&s_hist[L.stage], 1ull);
-        } else {
-          record_survivor(P, L, rcol, stride);
+        if (!PERSIST && status == kStRun && L.t - L.tseg >= P.step_cap) {
+          steps += (unsigned long long)(L.t - L.tseg);
+          L.tseg = L.t;
+          status = kStCap;
         }
-        status = kStIdle;
-        break;
-      }
-      if (!PERSIST && status == kStRun && L.t - L.tseg >= P.step_cap) {
-        steps += (unsigned long long)(L.t - L.tseg);
-        L.tseg = L.t;
-        status = kStCap;
       }
     }
   }
