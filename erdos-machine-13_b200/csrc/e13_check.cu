@@ -326,3 +326,85 @@ extern "C" int e13_check(e13_ctx *ctx, const e13_check_in *in, int n, int nmax, 
   cudaFree(d_out);
   return rc;
 }
+
+// ------------------------------------------------------------------------
+// The same check for callers that cannot allocate device memory.
+//
+// All device memory this entry point uses is fixed at load time: the tapes,
+// inputs and outputs of up to E13_CHECK_NOALLOC_MAX machines sit in the
+// file-scope arrays below (about 16 MB; every GPU that loads the library keeps
+// them until the process exits).  Host code cannot use these names as device
+// addresses, so the first call on each device looks the addresses up with
+// cudaGetSymbolAddress while that device is current and keeps them.
+
+namespace {
+
+constexpr i64 kNoAllocWords = (2 * kRecheckSide + 1 + 31) / 32 + 2;  // one recheck tape (cells -4e6 .. 4e6)
+
+static __device__ __align__(256) u32 g_noalloc_tapes[E13_CHECK_NOALLOC_MAX * kNoAllocWords];
+static __device__ __align__(256) e13_check_in g_noalloc_in[E13_CHECK_NOALLOC_MAX];
+static __device__ __align__(256) e13_check_out g_noalloc_out[E13_CHECK_NOALLOC_MAX];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocAddrs {
+  bool ready;
+  u32 *tapes;
+  e13_check_in *in;
+  e13_check_out *out;
+};
+NoAllocAddrs g_noalloc_addrs[kNoAllocMaxDevices];
+
+int noalloc_addresses(int device, NoAllocAddrs **out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return E13_ERR_ARG;
+  NoAllocAddrs &a = g_noalloc_addrs[device];
+  if (!a.ready) {
+    if (cudaGetSymbolAddress((void **)&a.tapes, g_noalloc_tapes) != cudaSuccess ||
+        cudaGetSymbolAddress((void **)&a.in, g_noalloc_in) != cudaSuccess ||
+        cudaGetSymbolAddress((void **)&a.out, g_noalloc_out) != cudaSuccess)
+      return E13_ERR_CUDA;
+    a.ready = true;
+  }
+  *out = &a;
+  return E13_OK;
+}
+
+}  // namespace
+
+extern "C" int e13_check_noalloc(int device, const e13_check_in *in, int n, int nmax, int mode, e13_check_out *out) {
+  if ((n > 0 && (!in || !out)) || n < 0 || nmax < 1 || nmax > E13_CHECK_MAX_NMAX ||
+      (mode != E13_CHECK_RECHECK && mode != E13_CHECK_DEEP))
+    return E13_ERR_ARG;
+  if (n > E13_CHECK_NOALLOC_MAX) return E13_ERR_NOALLOC_SIZE;
+  if (n == 0) return E13_OK;
+  if (cudaSetDevice(device) != cudaSuccess) return E13_ERR_CUDA;
+  NoAllocAddrs *a = nullptr;
+  int rc = noalloc_addresses(device, &a);
+  if (rc) return rc;
+  const bool deep = mode == E13_CHECK_DEEP;
+  const int W = (int)((kWinLeft + (1LL << nmax) + 4096 + 31) / 32 + 2);
+  const int nl = (int)std::min<i64>(32, kSmemBudget / ((i64)W * 4));
+  if (nl < 1) return E13_ERR_NOALLOC_SIZE;
+  const size_t smem = (size_t)W * nl * 4;
+  if (cudaFuncSetAttribute(check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return E13_ERR_CUDA;
+  // the arrays keep the previous call's contents: clear the tapes and outputs
+  if ((!deep && cudaMemset(a->tapes, 0, sizeof(u32) * (size_t)n * kNoAllocWords) != cudaSuccess) ||
+      cudaMemset(a->out, 0, sizeof(e13_check_out) * (size_t)n) != cudaSuccess ||
+      cudaMemcpy(a->in, in, sizeof(e13_check_in) * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess)
+    return E13_ERR_CUDA;
+  CheckParams P;
+  P.n = n;
+  P.nmax = nmax;
+  P.deep = deep ? 1 : 0;
+  P.W = W;
+  P.gwords = deep ? 0 : kNoAllocWords;
+  P.gshift = (kRecheckSide - kWinLeft) / 32;
+  P.gtapes = a->tapes;
+  P.in = a->in;
+  P.out = a->out;
+  check_kernel<<<(n + nl - 1) / nl, nl, smem>>>(P);
+  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+      cudaMemcpy(out, a->out, sizeof(e13_check_out) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return E13_ERR_CUDA;
+  return E13_OK;
+}

@@ -26,8 +26,9 @@ ERRORS = {
     -1: "bad argument", -2: "forced cells exceed FMAX", -3: "symmetric state named by a fixed cell or has one",
     -4: "start state in the symmetric states", -5: "CUDA error", -6: "frontier stack overflow",
     -7: "survivor buffer too small", -8: "too many states", -9: "cannot open machine file",
-    -10: "device wait timed out", -11: "no CUDA device",
+    -10: "device wait timed out", -11: "no CUDA device", -12: "more than the fixed no-allocation memory holds",
 }
+E13_CHECK_NOALLOC_MAX = 16
 
 
 class E13Error(RuntimeError):
@@ -126,6 +127,7 @@ def lib():
         L.e13_autotune.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Tuning), P(ctypes.c_double)]
         L.e13_run_full.argtypes = [ctypes.c_void_p, P(ctypes.c_int32), I, I, P(ctypes.c_int64)]
         L.e13_check.argtypes = [ctypes.c_void_p, P(CheckIn), I, I, I, P(CheckOut)]
+        L.e13_check_noalloc.argtypes = [I, P(CheckIn), I, I, I, P(CheckOut)]
         L.e13_raw_run.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int64, I,
                                   ctypes.c_int64, P(ctypes.c_int64), P(ctypes.c_uint64)]
         L.e13_parse_survivor_line.argtypes = [ctypes.c_char_p, P(CheckIn)]
@@ -138,7 +140,7 @@ def lib():
 EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine", "e13_setup",
             "e13_format_survivor", "e13_format_summary", "e13_default_tuning", "e13_ctx_create", "e13_ctx_destroy",
             "e13_search", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
-            "e13_format_recheck", "e13_format_deep", "e13_raw_run", "e13_autotune"]
+            "e13_format_recheck", "e13_format_deep", "e13_raw_run", "e13_autotune", "e13_check_noalloc"]
 
 
 def keys():
@@ -295,3 +297,15 @@ def format_deep(ci: CheckIn, o: CheckOut, nmax: int) -> str:
     buf = ctypes.create_string_buffer(8192)
     lib().e13_format_deep(ctypes.byref(ci), ctypes.byref(o), nmax, buf, 8192)
     return buf.value.decode()
+
+
+def check_noalloc(device: int, ins, nmax: int, mode: int = 0):
+    """e13_check_noalloc(): the deep check with no device allocation (at most
+    E13_CHECK_NOALLOC_MAX machines per call)."""
+    n = len(ins)
+    arr = (CheckIn * max(n, 1))(*ins)
+    out = (CheckOut * max(n, 1))()
+    r = lib().e13_check_noalloc(device, arr, n, nmax, mode, out)
+    if r:
+        raise E13Error(r, "e13_check_noalloc")
+    return [out[i] for i in range(n)]

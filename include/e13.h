@@ -42,7 +42,8 @@ enum {
   E13_ERR_NQ = -8,           /* more states than the device path supports (nq <= 16) */
   E13_ERR_IO = -9,           /* machine file missing or unreadable (src/e13search.c:113) */
   E13_ERR_TIMEOUT = -10,     /* a device wait ran out (bounded waits; no hang) */
-  E13_ERR_NO_DEVICE = -11    /* no CUDA device: there is no CPU fallback */
+  E13_ERR_NO_DEVICE = -11,   /* no CUDA device: there is no CPU fallback */
+  E13_ERR_NOALLOC_SIZE = -12 /* e13_check_noalloc: more machines (or a larger nmax) than its fixed memory holds */
 };
 
 /* A prepared candidate family: base machine with state X deleted.
@@ -240,6 +241,22 @@ typedef struct e13_check_out {
    recheck.c's step limit and tape (mode E13_CHECK_RECHECK, src/recheck.c:57-92)
    or deep.c's (E13_CHECK_DEEP, src/deep.c:49-80). */
 int e13_check(e13_ctx *ctx, const e13_check_in *in, int n, int nmax, int mode, e13_check_out *out);
+
+/* e13_check without any device allocation, for callers that cannot allocate:
+   a process whose GPU memory is all handed out by another allocator (a
+   framework's caching allocator or a fixed arena), or a latency-critical loop
+   that must not pay cudaMalloc/cudaFree's implicit device synchronisation.
+   This entry point has no counterpart in the reference.  The tapes, inputs and
+   outputs of at most E13_CHECK_NOALLOC_MAX machines live in fixed device
+   arrays compiled into the library (about 16 MB, held by every GPU that loads
+   it until the process exits); n above that returns E13_ERR_NOALLOC_SIZE.
+   in/out are host arrays of n entries, as for e13_check; the call is
+   synchronous on `device`.  Its first call on a device looks up the arrays'
+   device addresses (cudaGetSymbolAddress), so make that first call before any
+   stream capture.  All calls share the arrays: calls that overlap on the same
+   GPU (other host threads) race and must be serialised by the caller. */
+#define E13_CHECK_NOALLOC_MAX 16
+int e13_check_noalloc(int device, const e13_check_in *in, int n, int nmax, int mode, e13_check_out *out);
 
 /* Parses a SURVIVOR line into a checker input (src/recheck.c:28-56).
    Returns 1 on success, 0 if the line has no table. */
