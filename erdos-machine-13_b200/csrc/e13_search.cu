@@ -172,6 +172,9 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   u32 *tape = reinterpret_cast<u32 *>(keyc + 64);
   const int stride = blockDim.x;
   u32 *rows = tape + kTapeWords * stride;
+  // persistent: a shared-memory copy of each warp's current stack-top node, so
+  // lanes taking its children read shared memory instead of HBM
+  Node *mytop = reinterpret_cast<Node *>(rows + 16 * stride) + (threadIdx.x >> 5);
   __shared__ unsigned long long s_hist[kStages + 1];
   __shared__ unsigned long long s_leaves, s_steps;
 
@@ -259,6 +262,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
               else atomicOr(&ctl->error, kErrOutFull);
             }
             if (dst) lane_store(L, dst, tcol, rcol, stride, P.nq, fork_cell, keep, vm);
+            if (rank == npush - 1) lane_store(L, mytop, tcol, rcol, stride, P.nq, fork_cell, keep, vm);  // new top
           }
           if (npush > 0) {
             const int src = nth_bit64((u64)pm, npush - 1);  // lane holding the last node pushed on the warp stack
@@ -305,9 +309,11 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
       if (!im) break;
       if (!have_cur) {
         if (PERSIST && sp > 0) {
-          const Node *N = wst + wrap(wbot + sp - 1, D);
-          cur_keep = (N->flags & kFlagKeep) ? 1 : 0;
-          cur_vm = N->vmask;
+          // an older node is the top again: bring it into shared memory once
+          copy_node(mytop, wst + wrap(wbot + sp - 1, D), lane);
+          __syncwarp();
+          cur_keep = (mytop->flags & kFlagKeep) ? 1 : 0;
+          cur_vm = mytop->vmask;
           have_cur = true;
         } else {
           const Node *src = nullptr;
@@ -369,12 +375,16 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
           if (!src) break;
           if (PERSIST) {
             wbot = 0;
-            if (from_pool) copy_node_cg(wst, src, lane);
-            else copy_node(wst, src, lane);
+            if (lane < kNodeChunks) {
+              const uint4 v = from_pool ? __ldcg(reinterpret_cast<const uint4 *>(src) + lane)
+                                        : reinterpret_cast<const uint4 *>(src)[lane];
+              reinterpret_cast<uint4 *>(wst)[lane] = v;
+              reinterpret_cast<uint4 *>(mytop)[lane] = v;
+            }
             __syncwarp();
             sp = 1;
-            cur_keep = (wst->flags & kFlagKeep) ? 1 : 0;
-            cur_vm = wst->vmask;
+            cur_keep = (mytop->flags & kFlagKeep) ? 1 : 0;
+            cur_vm = mytop->vmask;
           } else {
             cur = src;
             cur_keep = (src->flags & kFlagKeep) ? 1 : 0;
@@ -384,7 +394,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
           backoff = 256;
         }
       }
-      const Node *N = PERSIST ? (wst + wrap(wbot + sp - 1, D)) : cur;
+      const Node *N = PERSIST ? mytop : cur;
       const int navail = cur_keep + __popcll(cur_vm);
       const int nidle = __popc(im);
       const int rank = __popc(im & lt_mask);
@@ -900,7 +910,7 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   P.surv = c->surv;
   P.ctl = c->ctl;
 
-  const size_t smem = kKeySmemBytes + (size_t)(kTapeWords + 16) * tu.block * 4;
+  const size_t smem = kKeySmemBytes + (size_t)(kTapeWords + 16) * tu.block * 4 + (size_t)(tu.block / 32) * sizeof(Node);
   if (persist) CK(cudaFuncSetAttribute(search_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   else CK(cudaFuncSetAttribute(search_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
