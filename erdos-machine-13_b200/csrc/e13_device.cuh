@@ -95,6 +95,21 @@ __constant__ u64 c_tgt[kStages + 2];
 __constant__ int c_deadline[kStages + 2];  // 4 * erdos_14 stage step + 64 (src/e13search.c:159)
 __constant__ int c_exc[kStages + 1];       // exceptions by stage (src/e13search.c:71)
 
+// Shared-memory copies of the stage tables: lanes of a warp index them by
+// their own stage, which constant memory would serialise.  Every kernel that
+// runs the filter fills them with load_stage_tables() before its first step.
+__shared__ u64 s_tgt[kStages + 2];
+__shared__ int s_deadline[kStages + 2];
+__shared__ int s_exc[kStages + 1];
+
+__device__ __forceinline__ void load_stage_tables() {
+  if (threadIdx.x < kStages + 2) {
+    s_tgt[threadIdx.x] = c_tgt[threadIdx.x];
+    s_deadline[threadIdx.x] = c_deadline[threadIdx.x];
+  }
+  if (threadIdx.x < kStages + 1) s_exc[threadIdx.x] = c_exc[threadIdx.x];
+}
+
 enum { kEvRun = 0, kEvDead = 1, kEvSurv = 2, kEvStage = 3, kEvCell = 4 };
 
 // Registers of one lane's machine.
@@ -221,37 +236,35 @@ __device__ __forceinline__ int lane_act(Lane &L, u32 *__restrict__ tcol, const u
   const u32 row = rcol[L.st * stride];
   const u32 sym = (word >> (p & 31)) & 1u;
   const u32 e = (row >> (sym << 4)) & 0x1FFu;
-  if (e & (kEntSpecial | kEntSelf)) {
-    if (e & kEntSpecial) {
-      cell = (L.st << 1) | (int)sym;
-      ecell = e & 0xFFu;
-      return kEvCell;
-    }
-    if (L.hb != L.tgt) {
-      // run skip (see step_slice): exact while hb, the state and the ones stay put
-      const bool right = (e & 2u) != 0;
-      int lim = L.deadline - L.t + 1;
-      const int room = right ? (kTapeCells - 2) - p : p - 1;
-      lim = lim < room ? lim : room;
-      if (lim > 1) {
-        const int k = run_length(tcol, stride, p, sym, right, lim);
-        if (k > 1) {
-          L.p = p + (right ? k : -k);
-          L.t += k;
-          return 0;
-        }
-      }
-    }
+  if (e & kEntSpecial) {
+    cell = (L.st << 1) | (int)sym;
+    ecell = e & 0xFFu;
+    return kEvCell;
   }
-  if ((e ^ sym) & 1u) {
-    tcol[widx] = word ^ (1u << (p & 31));
+  // k = steps of this action: 1, or on a self-loop cell (see step_slice) the
+  // rest of the run of sym inside this tape word, clamped by the deadline and
+  // the window.  Computed without branches so the warp does not split.
+  const bool right = (e & 2u) != 0;
+  const int b = p & 31;
+  const u32 x = word ^ (0u - sym);             // cells holding sym are 0 bits
+  const u32 xr = right ? x : __brev(x);        // look upwards in both directions
+  const int bb = right ? b : 31 - b;
+  const u32 up = xr >> bb;
+  int k = up ? __ffs(up) - 1 : 32 - bb;
+  const int lim_t = L.deadline - L.t + 1;
+  const int room = right ? (kTapeCells - 2) - p : p - 1;
+  k = k < lim_t ? k : lim_t;
+  k = k < room ? k : room;
+  k = ((e & kEntSelf) && L.hb != L.tgt && k > 1) ? k : 1;
+  if ((e ^ sym) & 1u) {  // never on a self-loop cell
+    tcol[widx] = word ^ (1u << b);
     L.hb ^= keyb[p];  // zero for cells < -2: those go to the counter hash
   }
-  const int np = p + (int)(e & 2u) - 1;
+  const int np = p + (right ? k : -k);
   if ((unsigned)(np - 1) >= (unsigned)(kTapeCells - 2)) return kEvDead;  // head <= -64 or >= 1299
   L.p = np;
   L.st = (int)((e >> 2) & 15u);
-  ++L.t;
+  L.t += k;
   if (L.hb == L.tgt) return stage_check(L, tcol, keyc, stride);
   return 0;
 }
@@ -275,7 +288,7 @@ __device__ __forceinline__ u64 counter_hash(const u32 *tcol, const u64 *keyc, in
 // The stage-start test of src/e13search.c:136-161 once hb matches TGT[nt].
 // Returns 0 (go on), kEvDead or kEvSurv.
 __device__ __forceinline__ int stage_check(Lane &L, const u32 *tcol, const u64 *keyc, int stride) {
-  const int nt = L.nt, c = c_exc[nt];
+  const int nt = L.nt, c = s_exc[nt];
   int a = L.flags & kFlagAbs, r = (L.flags >> 1) & 1;
   if (nt > 1) {
     if (L.st != L.st0) return 0;
@@ -301,8 +314,8 @@ __device__ __forceinline__ int stage_check(Lane &L, const u32 *tcol, const u64 *
   L.stage = nt;
   if (nt == kStages) return kEvSurv;
   L.nt = nt + 1;
-  L.deadline = c_deadline[nt + 1];
-  L.tgt = c_tgt[nt + 1];
+  L.deadline = s_deadline[nt + 1];
+  L.tgt = s_tgt[nt + 1];
   return 0;
 }
 

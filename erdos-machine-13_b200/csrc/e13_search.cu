@@ -80,7 +80,7 @@ __device__ __forceinline__ void lane_load(Lane &L, const Node *N, u32 *tcol, u32
   L.ch2 = N->ch[2];
   L.nintro = N->nintro;
   L.budget = N->budget;
-  L.tgt = c_tgt[L.nt];
+  L.tgt = s_tgt[L.nt];
   L.tseg = L.t;
   const uint4 *rv = reinterpret_cast<const uint4 *>(N->cellv);
   for (int k = 0; k < 4; ++k) {  // all 16 rows: states >= nq hold halts
@@ -185,6 +185,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
     s_leaves = 0;
     s_steps = 0;
   }
+  load_stage_tables();
   u32 *tcol = tape + threadIdx.x;
   u32 *rcol = rows + threadIdx.x;
   for (int w = 0; w < kTapeWords; ++w) tcol[w * stride] = 0;
@@ -218,6 +219,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   u64 cur_vm = 0;
   bool input_done = false;
   bool busy = false;           // persistent: counted in ctl->busy
+  bool top_dirty = false;      // persistent: the stack top lives only in the shared copy (its HBM slot is stale)
   int rounds = 0;              // slices run: a warp dumps only after one (progress every epoch)
   unsigned backoff = 256;
   unsigned long long st_lane_rounds = 0, st_polls = 0;
@@ -244,27 +246,35 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
         const bool more = (status == kStFork) && (keep || vm);
         const unsigned pm = __ballot_sync(kFull, more);
         if (pm) {
-          if (have_cur && sp > 0 && lane == 0) {
-            Node *t = wst + wrap(wbot + sp - 1, D);
-            t->vmask = cur_vm;
-            t->flags = (signed char)((t->flags & 31) | (cur_keep ? kFlagKeep : 0));
-          }
-          __syncwarp();
           const int rank = __popc(pm & lt_mask);
           const int npush = min(__popc(pm), D - sp);
+          if (npush > 0 && have_cur && sp > 0) {
+            // the current top goes under the new nodes: its HBM slot gets the
+            // shared copy (if that is newer) and the children still to run
+            Node *t = wst + wrap(wbot + sp - 1, D);
+            if (top_dirty) copy_node(t, mytop, lane);
+            __syncwarp();
+            if (lane == 0) {
+              t->vmask = cur_vm;
+              t->flags = (signed char)((t->flags & 31) | (cur_keep ? kFlagKeep : 0));
+            }
+          }
+          __syncwarp();
           if (more) {
             Node *dst = nullptr;
-            if (rank < npush) {
-              dst = wst + wrap(wbot + sp + rank, D);
+            if (rank < npush - 1) {
+              dst = wst + wrap(wbot + sp + rank, D);  // buried at once
+            } else if (rank == npush - 1) {
+              dst = mytop;  // the new top: kept in shared memory until it is buried
             } else {
               const unsigned long long k = atomicAdd(&ctl->nout, 1ull);
               if ((long long)k < P.out_cap) dst = P.out + k;
               else atomicOr(&ctl->error, kErrOutFull);
             }
             if (dst) lane_store(L, dst, tcol, rcol, stride, P.nq, fork_cell, keep, vm);
-            if (rank == npush - 1) lane_store(L, mytop, tcol, rcol, stride, P.nq, fork_cell, keep, vm);  // new top
           }
           if (npush > 0) {
+            top_dirty = true;
             const int src = nth_bit64((u64)pm, npush - 1);  // lane holding the last node pushed on the warp stack
             cur_keep = __shfl_sync(kFull, keep, src);
             const unsigned lo = __shfl_sync(kFull, (unsigned)vm, src);
@@ -312,6 +322,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
           // an older node is the top again: bring it into shared memory once
           copy_node(mytop, wst + wrap(wbot + sp - 1, D), lane);
           __syncwarp();
+          top_dirty = false;
           cur_keep = (mytop->flags & kFlagKeep) ? 1 : 0;
           cur_vm = mytop->vmask;
           have_cur = true;
@@ -383,6 +394,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
             }
             __syncwarp();
             sp = 1;
+            top_dirty = false;
             cur_keep = (mytop->flags & kFlagKeep) ? 1 : 0;
             cur_vm = mytop->vmask;
           } else {
@@ -408,6 +420,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
       __syncwarp();
       if (nidle >= navail) {
         have_cur = false;
+        top_dirty = false;
         if (PERSIST) --sp;
       } else {
         drop_children(cur_keep, cur_vm, nidle);
@@ -461,19 +474,22 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
           else atomicOr(&ctl->error, kErrOutFull);
           status = kStIdle;
         }
-        if (have_cur && sp > 0 && lane == 0) {
-          Node *t = wst + wrap(wbot + sp - 1, D);
-          t->vmask = cur_vm;
-          t->flags = (signed char)((t->flags & 31) | (cur_keep ? kFlagKeep : 0));
-        }
         __syncwarp();
         if (sp > 0) {
           unsigned long long base = 0;
           if (lane == 0) base = atomicAdd(&ctl->nout, (unsigned long long)sp);
           base = __shfl_sync(kFull, base, 0);
           for (int i = 0; i < sp; ++i) {
-            if ((long long)(base + i) < P.out_cap) copy_node(P.out + base + i, wst + wrap(wbot + i, D), lane);
+            const bool is_top = i == sp - 1;
+            const Node *from = (is_top && top_dirty) ? mytop : wst + wrap(wbot + i, D);
+            if ((long long)(base + i) < P.out_cap) copy_node(P.out + base + i, from, lane);
             else if (lane == 0) atomicOr(&ctl->error, kErrOutFull);
+          }
+          __syncwarp();
+          if (have_cur && lane == 0 && (long long)(base + sp - 1) < P.out_cap) {
+            Node *t = P.out + base + sp - 1;
+            t->vmask = cur_vm;
+            t->flags = (signed char)((t->flags & 31) | (cur_keep ? kFlagKeep : 0));
           }
         }
         if (busy && lane == 0) atomicSub(&ctl->busy, 1);
@@ -509,6 +525,8 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
       if (rm) {
 #pragma unroll 1
         for (int it = 0; it < P.slice; ++it) {
+          // end the slice early once a quarter of the lanes wait for work
+          if ((it & 7) == 7 && __popc(__ballot_sync(kFull, status == kStRun)) < 24) break;
           if (status == kStRun) {
             int cell = 0;
             u32 e = 0;
@@ -540,6 +558,10 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
               status = kStIdle;
             }
           }
+          // every lane comes here each iteration (the loop bounds and the early
+          // exit are warp-uniform): rejoin the lanes that took rare branches so
+          // the next action issues once for the whole warp
+          __syncwarp();
         }
         if (!PERSIST && status == kStRun && L.t - L.tseg >= P.step_cap) {
           steps += (unsigned long long)(L.t - L.tseg);
@@ -626,6 +648,7 @@ __global__ void __launch_bounds__(256) run_full_kernel(const int *tabs, int n, i
   u32 *rows = tape + kTapeWords * stride;
   for (int i = threadIdx.x; i < kTapeCells; i += stride) keyb[i] = (i >= kCounterCells) ? c_key[i] : 0ull;
   for (int i = threadIdx.x; i < 64; i += stride) keyc[i] = (i < kCounterCells) ? c_key[i] : 0ull;
+  load_stage_tables();
   __syncthreads();
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= n) return;
@@ -642,7 +665,7 @@ __global__ void __launch_bounds__(256) run_full_kernel(const int *tabs, int n, i
     rcol[s * stride] = cell_slot(2 * s, e0, true) | (cell_slot(2 * s + 1, e1, true) << 16);
   }
   Lane L;
-  L.p = kLeft; L.st = 0; L.t = 0; L.deadline = c_deadline[1]; L.hb = 0; L.tgt = c_tgt[1];
+  L.p = kLeft; L.st = 0; L.t = 0; L.deadline = s_deadline[1]; L.hb = 0; L.tgt = s_tgt[1];
   L.nt = 1; L.stage = 0; L.st0 = -1; L.p0 = kLeft; L.flags = 3; L.ch0 = L.ch1 = L.ch2 = 0;  // head0 = 0 until stage 1
   int ev;
   for (;;) {
