@@ -47,7 +47,7 @@ struct __align__(16) Node {
   int p, st, t, deadline;  // p = head + 64
   signed char nt, stage, st0, flags;
   short p0, pend;
-  unsigned char nintro, budget, pad0, pad1;
+  unsigned char nintro, budget, job, pad1;  // job: the slot of the search this machine belongs to
   u32 pad2[3];
   unsigned short cellv[32];  // cell entries with the self-loop bit; row s = cellv[2s] | cellv[2s+1] << 16
   u32 tape[kTapeWords];
@@ -62,8 +62,16 @@ constexpr int kNodeChunks = sizeof(Node) / 16;
 // Survivor record written by the device.
 struct SurvRec {
   unsigned char ent[32];
-  int st0, head0, abs_ok, rel_ok, t, pad[3];
+  int st0, head0, abs_ok, rel_ok, t, job, pad[2];
 };
+
+// Several searches ("jobs") can share one persistent kernel: every node, lane
+// and survivor record carries its job's slot.  Per-job constants and counters:
+constexpr int kMaxJobs = 16;
+struct JobParam {
+  int nv, sym_lo, sym_hi, pad;  // 4 * nq moves; relabel-symmetry range (-1: off)
+};
+constexpr int kJobCounters = 2 + kStages + 1;  // leaves, steps, deaths by stage 0..9
 
 // Control block of one search (device memory).
 struct Ctl {
@@ -77,8 +85,6 @@ struct Ctl {
   int busy;                      // persistent: warps holding work or claiming it
   int error;                     // kErr* bits
   int launches;
-  u64 leaves, steps;
-  u64 hist[kStages + 1];
   // utilisation counters: warp rounds, running lanes summed over rounds,
   // pool donations and claims, idle-warp polls
   u64 rounds, lane_rounds, donations, claims, polls;
@@ -114,7 +120,7 @@ enum { kEvRun = 0, kEvDead = 1, kEvSurv = 2, kEvStage = 3, kEvCell = 4 };
 
 // Registers of one lane's machine.
 struct Lane {
-  int p, st, t, deadline, tseg;
+  int p, st, t, deadline, tseg, job;
   u64 hb, tgt;
   int nt, stage, st0, p0, flags;
   u64 ch0, ch1, ch2;

@@ -44,7 +44,9 @@ constexpr long long kPoolNodes = 1LL << 18;  // donation pool: 256 Ki nodes (80 
 // steps a lane gets between warp-level refill rounds is Params::slice
 
 struct Params {
-  int nq, nv, sym_lo, sym_hi;
+  const JobParam *jobs;      // kMaxJobs entries
+  unsigned long long *jobcnt;  // kMaxJobs x kJobCounters totals
+  int nq;
   int slice, step_cap, wdepth, pool_low, run_skip;
   long long out_cap, out_soft, surv_cap, pool_cap;
   long long epoch_ns;
@@ -80,6 +82,7 @@ __device__ __forceinline__ void lane_load(Lane &L, const Node *N, u32 *tcol, u32
   L.ch2 = N->ch[2];
   L.nintro = N->nintro;
   L.budget = N->budget;
+  L.job = N->job;
   L.tgt = s_tgt[L.nt];
   L.tseg = L.t;
   const uint4 *rv = reinterpret_cast<const uint4 *>(N->cellv);
@@ -113,6 +116,7 @@ __device__ __forceinline__ void lane_store(const Lane &L, Node *N, const u32 *tc
   N->pend = (short)pend;
   N->nintro = (unsigned char)L.nintro;
   N->budget = (unsigned char)L.budget;
+  N->job = (unsigned char)L.job;
   uint4 *rv = reinterpret_cast<uint4 *>(N->cellv);
   for (int k = 0; k < 4; ++k)
     rv[k] = make_uint4(rcol[(4 * k) * stride], rcol[(4 * k + 1) * stride], rcol[(4 * k + 2) * stride],
@@ -153,6 +157,7 @@ __device__ __forceinline__ void record_survivor(const Params &P, const Lane &L, 
   r->abs_ok = L.flags & 1;
   r->rel_ok = (L.flags >> 1) & 1;
   r->t = L.t;
+  r->job = L.job;
 }
 
 enum { kStRun = 0, kStIdle = 1, kStFork = 2, kStCap = 3 };
@@ -175,16 +180,16 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   // persistent: a shared-memory copy of each warp's current stack-top node, so
   // lanes taking its children read shared memory instead of HBM
   Node *mytop = reinterpret_cast<Node *>(rows + 16 * stride) + (threadIdx.x >> 5);
-  __shared__ unsigned long long s_hist[kStages + 1];
-  __shared__ unsigned long long s_leaves, s_steps;
+  __shared__ int4 s_jp[kMaxJobs];                              // per-job moves and symmetry range
+  __shared__ unsigned long long s_jc[kMaxJobs][kJobCounters];  // per-job leaves, steps, deaths by stage
 
   for (int i = threadIdx.x; i < kTapeCells; i += stride) keyb[i] = (i >= kCounterCells) ? c_key[i] : 0ull;
   for (int i = threadIdx.x; i < 64; i += stride) keyc[i] = (i < kCounterCells) ? c_key[i] : 0ull;
-  if (threadIdx.x <= kStages) s_hist[threadIdx.x] = 0;
-  if (threadIdx.x == 0) {
-    s_leaves = 0;
-    s_steps = 0;
+  if (threadIdx.x < kMaxJobs) {
+    const JobParam jp = P.jobs[threadIdx.x];
+    s_jp[threadIdx.x] = make_int4(jp.nv, jp.sym_lo, jp.sym_hi, 0);
   }
+  for (int i = threadIdx.x; i < kMaxJobs * kJobCounters; i += stride) (&s_jc[0][0])[i] = 0ull;
   load_stage_tables();
   u32 *tcol = tape + threadIdx.x;
   u32 *rcol = rows + threadIdx.x;
@@ -208,8 +213,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   int status = kStIdle;
   int fork_cell = 0;
   u32 fork_e = 0;
-  unsigned leaves = 0;
-  unsigned long long steps = 0;
+  L.job = 0;
 
   // warp-uniform state
   int sp = 0, wbot = 0;        // persistent: this warp's DFS stack, a ring of D slots from wbot
@@ -230,7 +234,10 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
     if (__any_sync(kFull, status == kStFork)) {
       int keep = 0;
       u64 vm = 0;
-      if (status == kStFork) child_set(fork_e, L.budget, L.nintro, P.nv, P.sym_lo, P.sym_hi, keep, vm);
+      if (status == kStFork) {
+        const int4 jp = s_jp[L.job];
+        child_set(fork_e, L.budget, L.nintro, jp.x, jp.y, jp.z, keep, vm);
+      }
       if (PERSIST) {
         // the forking lane goes on with the first child in place; the rest is pushed
         int first = -2;
@@ -290,7 +297,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
             set_entry(rcol, stride, fork_cell, fork_e & 0x7Fu, P.run_skip);
           } else {
             if (fork_e != kEntFree) L.budget -= 1;
-            L.nintro = sym_after(first, L.nintro, P.sym_lo, P.sym_hi);
+            L.nintro = sym_after(first, L.nintro, s_jp[L.job].y, s_jp[L.job].z);
             set_entry(rcol, stride, fork_cell, (u32)first, P.run_skip);
           }
           status = kStRun;
@@ -414,7 +421,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
         int ch = -1;
         if (!(cur_keep && rank == 0)) ch = nth_bit64(cur_vm, rank - cur_keep);
         lane_load(L, N, tcol, rcol, stride, P.nq);
-        apply_child(L, N, ch, rcol, stride, P.sym_lo, P.sym_hi, P.run_skip);
+        apply_child(L, N, ch, rcol, stride, s_jp[N->job].y, s_jp[N->job].z, P.run_skip);
         status = kStRun;
       }
       __syncwarp();
@@ -467,7 +474,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
       if (d && rounds > 0) {
         // dump: live lanes as resume nodes, then this warp's stack
         if (status == kStRun) {
-          steps += (unsigned long long)(L.t - L.tseg);
+          atomicAdd(&s_jc[L.job][1], (unsigned long long)(L.t - L.tseg));
           L.tseg = L.t;
           const unsigned long long k = atomicAdd(&ctl->nout, 1ull);
           if ((long long)k < P.out_cap) lane_store(L, P.out + k, tcol, rcol, stride, P.nq, -1, 1, 0ull);
@@ -536,7 +543,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
                 ev = kEvDead;
               } else if (e == kEntFree || L.budget > 0) {
                 // a fork: handled by the warp at the next round
-                steps += (unsigned long long)(L.t - L.tseg);
+                atomicAdd(&s_jc[L.job][1], (unsigned long long)(L.t - L.tseg));
                 L.tseg = L.t;
                 fork_cell = cell;
                 fork_e = e;
@@ -550,10 +557,10 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
             }
             if (ev) {
               // a leaf
-              steps += (unsigned long long)(L.t - L.tseg);
+              atomicAdd(&s_jc[L.job][1], (unsigned long long)(L.t - L.tseg));
               L.tseg = L.t;
-              ++leaves;
-              if (ev == kEvDead) atomicAdd(&s_hist[L.stage], 1ull);
+              atomicAdd(&s_jc[L.job][0], 1ull);
+              if (ev == kEvDead) atomicAdd(&s_jc[L.job][2 + L.stage], 1ull);
               else record_survivor(P, L, rcol, stride);
               status = kStIdle;
             }
@@ -564,7 +571,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
           __syncwarp();
         }
         if (!PERSIST && status == kStRun && L.t - L.tseg >= P.step_cap) {
-          steps += (unsigned long long)(L.t - L.tseg);
+          atomicAdd(&s_jc[L.job][1], (unsigned long long)(L.t - L.tseg));
           L.tseg = L.t;
           status = kStCap;
         }
@@ -573,14 +580,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   }
 
   // ---- totals
-  unsigned long long wl = leaves, ws = steps;
-  for (int o = 16; o > 0; o >>= 1) {
-    wl += __shfl_down_sync(kFull, wl, o);
-    ws += __shfl_down_sync(kFull, ws, o);
-  }
   if (lane == 0) {
-    atomicAdd(&s_leaves, wl);
-    atomicAdd(&s_steps, ws);
     atomicAdd(&ctl->rounds, (unsigned long long)rounds);
     atomicAdd(&ctl->lane_rounds, st_lane_rounds);
     atomicAdd(&ctl->polls, st_polls);
@@ -588,11 +588,24 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
     if (st_claims) atomicAdd(&ctl->claims, (unsigned long long)st_claims);
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    atomicAdd(&ctl->leaves, s_leaves);
-    atomicAdd(&ctl->steps, s_steps);
+  for (int i = threadIdx.x; i < kMaxJobs * kJobCounters; i += stride) {
+    const unsigned long long v = (&s_jc[0][0])[i];
+    if (v) atomicAdd(P.jobcnt + i, v);
   }
-  if (threadIdx.x <= kStages && s_hist[threadIdx.x]) atomicAdd(&ctl->hist[threadIdx.x], s_hist[threadIdx.x]);
+}
+
+// Live nodes of each job on the frontier stack.  Between launches every
+// unfinished machine of the persistent kernel is there, so a job whose count
+// is zero is finished.
+__global__ void count_job_nodes(const Ctl *ctl, const Node *stack, unsigned long long *counts) {
+  __shared__ unsigned int s_n[kMaxJobs];
+  if (threadIdx.x < kMaxJobs) s_n[threadIdx.x] = 0;
+  __syncthreads();
+  const long long top = ctl->top;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < top; i += (long long)gridDim.x * blockDim.x)
+    atomicAdd(&s_n[stack[i].job & (kMaxJobs - 1)], 1u);
+  __syncthreads();
+  if (threadIdx.x < kMaxJobs && s_n[threadIdx.x]) atomicAdd(&counts[threadIdx.x], (unsigned long long)s_n[threadIdx.x]);
 }
 
 // Between launches: the input taken from the top of the stack is gone; the
@@ -714,6 +727,10 @@ struct e13_ctx {
   long long surv_cap;
   Ctl *ctl;
   Ctl *ctl_host;
+  JobParam *d_jobs;              // kMaxJobs
+  unsigned long long *d_jobcnt;  // kMaxJobs x kJobCounters
+  unsigned long long *d_jobnodes;  // kMaxJobs
+  unsigned long long *h_jobbuf;  // pinned: counters then node counts
   e13_stats stats;
 };
 
@@ -765,6 +782,10 @@ extern "C" int e13_ctx_create(int device, e13_ctx **out) {
   CK(cudaEventCreate(&c->k1));
   CK(cudaMallocHost(&c->ctl_host, sizeof(Ctl)));
   CK(cudaMalloc(&c->ctl, sizeof(Ctl)));
+  CK(cudaMalloc(&c->d_jobs, sizeof(JobParam) * kMaxJobs));
+  CK(cudaMalloc(&c->d_jobcnt, sizeof(unsigned long long) * kMaxJobs * kJobCounters));
+  CK(cudaMalloc(&c->d_jobnodes, sizeof(unsigned long long) * kMaxJobs));
+  CK(cudaMallocHost(&c->h_jobbuf, sizeof(unsigned long long) * kMaxJobs * (kJobCounters + 1)));
   *out = c;
   return E13_OK;
 }
@@ -781,6 +802,10 @@ extern "C" void e13_ctx_destroy(e13_ctx *c) {
   cudaFree(c->surv);
   cudaFree(c->ctl);
   cudaFreeHost(c->ctl_host);
+  cudaFree(c->d_jobs);
+  cudaFree(c->d_jobcnt);
+  cudaFree(c->d_jobnodes);
+  cudaFreeHost(c->h_jobbuf);
   cudaEventDestroy(c->ev0);
   cudaEventDestroy(c->ev1);
   cudaEventDestroy(c->k0);
@@ -815,8 +840,9 @@ static int grow(T **p, long long *cap, long long want) {
   return E13_OK;
 }
 
-static void build_root(const e13_job *job, Node *root) {
+static void build_root(const e13_job *job, int slot, Node *root) {
   memset(root, 0, sizeof *root);
+  root->job = (unsigned char)slot;
   root->p = kLeft;
   root->deadline = 4 * 2 + 64;
   root->nt = 1;
@@ -910,11 +936,17 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   const long long scap = std::max<long long>(surv_cap, 1024);
   if ((rc = grow(&c->surv, &c->surv_cap, scap))) return rc;
 
+  JobParam jp[kMaxJobs];
+  memset(jp, 0, sizeof jp);
+  jp[0].nv = 4 * job->nq;
+  jp[0].sym_lo = job->sym_lo;
+  jp[0].sym_hi = job->sym_hi;
+  CK(cudaMemcpyAsync(c->d_jobs, jp, sizeof jp, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->d_jobcnt, 0, sizeof(unsigned long long) * kMaxJobs * kJobCounters, c->stream));
   Params P;
+  P.jobs = c->d_jobs;
+  P.jobcnt = c->d_jobcnt;
   P.nq = job->nq;
-  P.nv = 4 * job->nq;
-  P.sym_lo = job->sym_lo;
-  P.sym_hi = job->sym_hi;
   P.slice = tu.slice;
   P.run_skip = tu.run_skip ? 1 : 0;
   P.step_cap = tu.step_cap;
@@ -939,7 +971,7 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
 
   // the root: blank tape, every cell unread
   Node root;
-  build_root(job, &root);
+  build_root(job, 0, &root);
   memset(c->ctl_host, 0, sizeof(Ctl));
   c->ctl_host->top = 1;
   c->ctl_host->batch = 1;
@@ -1022,11 +1054,12 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   if (err) return err;
 
   const Ctl &h = *c->ctl_host;
+  CK(cudaMemcpy(c->h_jobbuf, c->d_jobcnt, sizeof(unsigned long long) * kJobCounters, cudaMemcpyDeviceToHost));
   memset(counts, 0, sizeof *counts);
-  counts->leaves = h.leaves;
-  counts->steps = h.steps;
+  counts->leaves = c->h_jobbuf[0];
+  counts->steps = c->h_jobbuf[1];
   counts->survivors = h.nsurv;
-  for (int j = 0; j <= E13_STAGES; ++j) counts->hist[j] = h.hist[j];
+  for (int j = 0; j <= E13_STAGES; ++j) counts->hist[j] = c->h_jobbuf[2 + j];
   const long long ns = (long long)h.nsurv;
   *nsurv = (int)std::min<long long>(ns, 0x7FFFFFFF);
   const long long ncopy = std::min<long long>(ns, std::min<long long>(surv_cap, c->surv_cap));
@@ -1110,5 +1143,275 @@ extern "C" int e13_autotune(e13_ctx *c, const e13_job *job, const e13_tuning *st
   }
   *best = cur;
   if (best_ms) *best_ms = cur_ms;
+  return E13_OK;
+}
+
+// ------------------------------------------------------------------------
+// serving: many searches in one persistent kernel (continuous batching)
+
+#include <chrono>
+#include <deque>
+#include <memory>
+#include <unordered_map>
+
+namespace {
+
+struct ServeJob {
+  int64_t id;
+  e13_job job;
+  double t_submit, t_start;
+  int slot;
+  std::vector<e13_survivor> surv;
+};
+
+double wall_seconds() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+struct e13_serve {
+  e13_ctx *c;
+  e13_tuning tu;
+  Params P;
+  size_t smem;
+  long long batch_max, out_nodes, reserve;
+  std::deque<std::unique_ptr<ServeJob>> queue;
+  std::unique_ptr<ServeJob> slot_job[kMaxJobs];
+  std::unordered_map<int64_t, std::vector<e13_survivor>> finished_surv;
+  JobParam jp[kMaxJobs];
+  unsigned long long surv_fetched;
+  bool surv_overflow;
+  double t0;
+  double device_ms;
+  long long epochs;
+};
+
+extern "C" int e13_serve_create(e13_ctx *c, const e13_tuning *tuning, int64_t reserve_nodes, e13_serve **out) {
+  if (!c || !out) return E13_ERR_ARG;
+  *out = nullptr;
+  e13_tuning tu;
+  e13_default_tuning(&tu);
+  tu.epoch_us = 20000;  // short epochs: new jobs join at every epoch boundary
+  if (tuning) {
+    if (tuning->block) tu.block = tuning->block;
+    if (tuning->slice) tu.slice = tuning->slice;
+    if (tuning->warp_stack) tu.warp_stack = tuning->warp_stack;
+    if (tuning->epoch_us) tu.epoch_us = tuning->epoch_us;
+    if (tuning->pool_low_pct) tu.pool_low_pct = tuning->pool_low_pct;
+    tu.run_skip = tuning->run_skip;
+    if (tuning->stack_nodes) tu.stack_nodes = tuning->stack_nodes;
+  }
+  tu.kernel = E13_KERNEL_PERSISTENT;
+  if (tu.block < 64 || tu.block > 768 || tu.block % 32 || tu.slice < 1 || tu.warp_stack < 1) return E13_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  int rc = ensure_consts(c);
+  if (rc) return rc;
+  std::unique_ptr<e13_serve> s(new e13_serve());
+  s->c = c;
+  s->tu = tu;
+  const long long nwarps = (long long)c->nsm * tu.block / 32;
+  const long long dump_room = nwarps * (32 + tu.warp_stack);
+  s->batch_max = nwarps * 16;
+  s->out_nodes = 2 * dump_room + 65536;
+  s->reserve = reserve_nodes > 0 ? reserve_nodes : (1LL << 18);
+  const long long stack_nodes = tu.stack_nodes > 0 ? tu.stack_nodes : (4LL << 20);
+  if ((rc = grow(&c->stack, &c->stack_cap, stack_nodes))) return rc;
+  if ((rc = grow(&c->out, &c->out_cap, s->out_nodes))) return rc;
+  if ((rc = grow(&c->wstack, &c->wstack_nodes, nwarps * tu.warp_stack))) return rc;
+  if ((rc = grow(&c->pool, &c->pool_cap, kPoolNodes))) return rc;
+  if ((rc = grow(&c->pool_ready, &c->pool_ready_cap, kPoolNodes))) return rc;
+  if ((rc = grow(&c->surv, &c->surv_cap, 1LL << 20))) return rc;
+  memset(s->jp, 0, sizeof s->jp);
+  Params &P = s->P;
+  P.jobs = c->d_jobs;
+  P.jobcnt = c->d_jobcnt;
+  P.nq = 16;
+  P.slice = tu.slice;
+  P.run_skip = tu.run_skip ? 1 : 0;
+  P.step_cap = tu.step_cap;
+  P.wdepth = tu.warp_stack;
+  P.pool_low = (int)std::max<long long>(1, nwarps * tu.pool_low_pct / 100);
+  P.pool_cap = c->pool_cap;
+  P.pool = c->pool;
+  P.pool_ready = c->pool_ready;
+  P.out_cap = c->out_cap;
+  P.out_soft = c->out_cap - dump_room - 1024;
+  P.surv_cap = c->surv_cap;
+  P.epoch_ns = (long long)tu.epoch_us * 1000LL;
+  P.stack = c->stack;
+  P.out = c->out;
+  P.wstack = c->wstack;
+  P.surv = c->surv;
+  P.ctl = c->ctl;
+  s->smem = kKeySmemBytes + (size_t)(kTapeWords + 16) * tu.block * 4 + (size_t)(tu.block / 32) * sizeof(Node);
+  CK(cudaFuncSetAttribute(search_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem));
+  memset(c->ctl_host, 0, sizeof(Ctl));
+  CK(cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->pool_ready, 0, sizeof(int) * (size_t)c->pool_ready_cap, c->stream));
+  CK(cudaMemsetAsync(c->d_jobcnt, 0, sizeof(unsigned long long) * kMaxJobs * kJobCounters, c->stream));
+  CK(cudaMemcpyAsync(c->d_jobs, s->jp, sizeof s->jp, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  s->t0 = wall_seconds();
+  *out = s.release();
+  return E13_OK;
+}
+
+extern "C" void e13_serve_destroy(e13_serve *s) { delete s; }
+
+extern "C" double e13_serve_clock(const e13_serve *s) { return s ? wall_seconds() - s->t0 : 0.0; }
+
+extern "C" int e13_serve_submit(e13_serve *s, const e13_job *job, int64_t id, double t_submit) {
+  if (!s || !job) return E13_ERR_ARG;
+  if (job->nq < 1 || job->nq > 16) return E13_ERR_NQ;
+  if (job->budget < 0) return E13_ERR_FMAX;
+  for (int i = 0; i < 2 * job->nq; ++i)
+    if (job->tab[i] < E13_FREE || (job->tab[i] >= 0 && (job->tab[i] >> 2) >= job->nq)) return E13_ERR_ARG;
+  std::unique_ptr<ServeJob> j(new ServeJob());
+  j->id = id;
+  j->job = *job;
+  j->t_submit = t_submit >= 0 ? t_submit : e13_serve_clock(s);
+  j->t_start = -1;
+  j->slot = -1;
+  s->queue.push_back(std::move(j));
+  return E13_OK;
+}
+
+extern "C" int64_t e13_serve_pending(const e13_serve *s) {
+  if (!s) return 0;
+  int64_t n = (int64_t)s->queue.size();
+  for (int k = 0; k < kMaxJobs; ++k) n += s->slot_job[k] ? 1 : 0;
+  return n;
+}
+
+extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int *ndone) {
+  if (!s || !ndone || (cap > 0 && !done) || cap < kMaxJobs) return E13_ERR_ARG;
+  *ndone = 0;
+  e13_ctx *c = s->c;
+  CK(cudaSetDevice(c->device));
+  const double now = e13_serve_clock(s);
+  // 1. admission: a free slot, the job's arrival time passed, and frontier room
+  //    for every running job's reservation plus this one
+  int running = 0;
+  for (int k = 0; k < kMaxJobs; ++k) running += s->slot_job[k] ? 1 : 0;
+  long long top = c->ctl_host->top;
+  std::vector<Node> roots;
+  while (!s->queue.empty() && s->queue.front()->t_submit <= now) {
+    int slot = -1;
+    for (int k = 0; k < kMaxJobs && slot < 0; ++k)
+      if (!s->slot_job[k]) slot = k;
+    if (slot < 0) break;
+    const long long need = top + (long long)roots.size() + s->reserve * (running + 1) + s->out_nodes;
+    if (need > c->stack_cap) break;
+    std::unique_ptr<ServeJob> j = std::move(s->queue.front());
+    s->queue.pop_front();
+    j->slot = slot;
+    j->t_start = now;
+    s->jp[slot].nv = 4 * j->job.nq;
+    s->jp[slot].sym_lo = j->job.sym_lo;
+    s->jp[slot].sym_hi = j->job.sym_hi;
+    Node root;
+    build_root(&j->job, slot, &root);
+    roots.push_back(root);
+    CK(cudaMemsetAsync(c->d_jobcnt + (size_t)slot * kJobCounters, 0, sizeof(unsigned long long) * kJobCounters,
+                       c->stream));
+    s->slot_job[slot] = std::move(j);
+    ++running;
+  }
+  if (!roots.empty()) {
+    CK(cudaMemcpyAsync(c->stack + top, roots.data(), sizeof(Node) * roots.size(), cudaMemcpyHostToDevice, c->stream));
+    top += (long long)roots.size();
+    long long tb[2] = {top, std::min(top, s->batch_max)};
+    CK(cudaMemcpyAsync(c->ctl, tb, sizeof tb, cudaMemcpyHostToDevice, c->stream));  // Ctl::top, Ctl::batch
+    CK(cudaMemcpyAsync(c->d_jobs, s->jp, sizeof s->jp, cudaMemcpyHostToDevice, c->stream));
+    c->ctl_host->top = top;
+  }
+  if (running == 0) return E13_OK;
+  // 2. one epoch of the persistent kernel, then the live nodes of every job
+  CK(cudaEventRecord(c->k0, c->stream));
+  search_kernel<true><<<c->nsm, s->tu.block, s->smem, c->stream>>>(s->P);
+  move_outputs<<<c->nsm * 4, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, c->stack_cap);
+  finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, s->batch_max, c->pool_cap);
+  CK(cudaMemsetAsync(c->d_jobnodes, 0, sizeof(unsigned long long) * kMaxJobs, c->stream));
+  count_job_nodes<<<c->nsm * 2, 256, 0, c->stream>>>(c->ctl, c->stack, c->d_jobnodes);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->k1, c->stream));
+  CK(cudaMemcpyAsync(c->ctl_host, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->h_jobbuf, c->d_jobcnt, sizeof(unsigned long long) * kMaxJobs * kJobCounters,
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->h_jobbuf + kMaxJobs * kJobCounters, c->d_jobnodes, sizeof(unsigned long long) * kMaxJobs,
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->k0, c->k1);
+  s->device_ms += ms;
+  s->epochs += 1;
+  if (c->ctl_host->error) return (c->ctl_host->error & kErrTimeout) ? E13_ERR_TIMEOUT : E13_ERR_OVERFLOW;
+  // 3. survivors found in this epoch go to their jobs
+  const unsigned long long ns = c->ctl_host->nsurv;
+  const unsigned long long avail = std::min<unsigned long long>(ns, (unsigned long long)c->surv_cap);
+  if (ns > (unsigned long long)c->surv_cap) s->surv_overflow = true;
+  if (avail > s->surv_fetched) {
+    std::vector<SurvRec> recs((size_t)(avail - s->surv_fetched));
+    CK(cudaMemcpy(recs.data(), c->surv + s->surv_fetched, sizeof(SurvRec) * recs.size(), cudaMemcpyDeviceToHost));
+    for (const SurvRec &r : recs) {
+      ServeJob *j = (r.job >= 0 && r.job < kMaxJobs) ? s->slot_job[r.job].get() : nullptr;
+      if (!j) continue;
+      e13_survivor sv;
+      decode_survivor(r, j->job.nq, &sv);
+      j->surv.push_back(sv);
+    }
+    s->surv_fetched = avail;
+  }
+  // 4. jobs with no node left are done
+  const double tdone = e13_serve_clock(s);
+  const unsigned long long *cnt = c->h_jobbuf, *nodes = c->h_jobbuf + kMaxJobs * kJobCounters;
+  for (int k = 0; k < kMaxJobs; ++k) {
+    if (!s->slot_job[k] || nodes[k] != 0) continue;
+    ServeJob &j = *s->slot_job[k];
+    e13_serve_result &r = done[(*ndone)++];
+    memset(&r, 0, sizeof r);
+    r.id = j.id;
+    r.counts.leaves = cnt[k * kJobCounters + 0];
+    r.counts.steps = cnt[k * kJobCounters + 1];
+    for (int h = 0; h <= E13_STAGES; ++h) r.counts.hist[h] = cnt[k * kJobCounters + 2 + h];
+    r.counts.survivors = (uint64_t)j.surv.size();
+    r.nsurv = (int32_t)j.surv.size();
+    r.status = s->surv_overflow ? E13_ERR_SURV_CAP : E13_OK;
+    r.t_submit = j.t_submit;
+    r.t_start = j.t_start;
+    r.t_done = tdone;
+    s->finished_surv[j.id] = std::move(j.surv);
+    s->slot_job[k].reset();
+  }
+  // 5. idle: start the survivor buffer over
+  if (e13_serve_pending(s) == 0) {
+    unsigned long long zero = 0;
+    CK(cudaMemcpyAsync(&c->ctl->nsurv, &zero, sizeof zero, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    s->surv_fetched = 0;
+    s->surv_overflow = false;
+    c->ctl_host->nsurv = 0;
+  }
+  return E13_OK;
+}
+
+extern "C" int e13_serve_survivors(e13_serve *s, int64_t id, e13_survivor *out, int cap, int *n) {
+  if (!s || !n || (cap > 0 && !out)) return E13_ERR_ARG;
+  auto it = s->finished_surv.find(id);
+  if (it == s->finished_surv.end()) return E13_ERR_ARG;
+  const int k = (int)std::min<size_t>(it->second.size(), (size_t)std::max(cap, 0));
+  for (int i = 0; i < k; ++i) out[i] = it->second[(size_t)i];
+  *n = (int)it->second.size();
+  const int rc = (size_t)k < it->second.size() ? E13_ERR_SURV_CAP : E13_OK;
+  s->finished_surv.erase(it);
+  return rc;
+}
+
+extern "C" int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs) {
+  if (!s) return E13_ERR_ARG;
+  if (device_ms) *device_ms = s->device_ms;
+  if (epochs) *epochs = s->epochs;
   return E13_OK;
 }

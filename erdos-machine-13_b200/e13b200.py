@@ -72,6 +72,11 @@ class Stats(ctypes.Structure):
                 ("idle_polls", ctypes.c_int64)]
 
 
+class ServeResult(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_int64), ("status", ctypes.c_int32), ("nsurv", ctypes.c_int32), ("counts", Counts),
+                ("t_submit", ctypes.c_double), ("t_start", ctypes.c_double), ("t_done", ctypes.c_double)]
+
+
 E13_CHECK_MAX_NMAX = 20
 E13_CHECK_MAX_ONES = 64
 
@@ -125,6 +130,17 @@ def lib():
         L.e13_search.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Counts), P(Survivor), I, P(I)]
         L.e13_last_stats.argtypes = [ctypes.c_void_p, P(Stats)]
         L.e13_autotune.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Tuning), P(ctypes.c_double)]
+        L.e13_serve_create.argtypes = [ctypes.c_void_p, P(Tuning), ctypes.c_int64, P(ctypes.c_void_p)]
+        L.e13_serve_destroy.argtypes = [ctypes.c_void_p]
+        L.e13_serve_destroy.restype = None
+        L.e13_serve_clock.argtypes = [ctypes.c_void_p]
+        L.e13_serve_clock.restype = ctypes.c_double
+        L.e13_serve_submit.argtypes = [ctypes.c_void_p, P(Job), ctypes.c_int64, ctypes.c_double]
+        L.e13_serve_step.argtypes = [ctypes.c_void_p, P(ServeResult), I, P(I)]
+        L.e13_serve_pending.argtypes = [ctypes.c_void_p]
+        L.e13_serve_pending.restype = ctypes.c_int64
+        L.e13_serve_survivors.argtypes = [ctypes.c_void_p, ctypes.c_int64, P(Survivor), I, P(I)]
+        L.e13_serve_stats.argtypes = [ctypes.c_void_p, P(ctypes.c_double), P(ctypes.c_int64)]
         L.e13_run_full.argtypes = [ctypes.c_void_p, P(ctypes.c_int32), I, I, P(ctypes.c_int64)]
         L.e13_check.argtypes = [ctypes.c_void_p, P(CheckIn), I, I, I, P(CheckOut)]
         L.e13_check_noalloc.argtypes = [I, P(CheckIn), I, I, I, P(CheckOut)]
@@ -140,7 +156,9 @@ def lib():
 EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine", "e13_setup",
             "e13_format_survivor", "e13_format_summary", "e13_default_tuning", "e13_ctx_create", "e13_ctx_destroy",
             "e13_search", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
-            "e13_format_recheck", "e13_format_deep", "e13_raw_run", "e13_autotune", "e13_check_noalloc"]
+            "e13_format_recheck", "e13_format_deep", "e13_raw_run", "e13_autotune", "e13_check_noalloc",
+            "e13_serve_create", "e13_serve_destroy", "e13_serve_clock", "e13_serve_submit", "e13_serve_step",
+            "e13_serve_pending", "e13_serve_survivors", "e13_serve_stats"]
 
 
 def keys():
@@ -309,3 +327,68 @@ def check_noalloc(device: int, ins, nmax: int, mode: int = 0):
     if r:
         raise E13Error(r, "e13_check_noalloc")
     return [out[i] for i in range(n)]
+
+
+class Server:
+    """Continuous batching of search jobs in one persistent kernel (e13_serve_*)."""
+
+    def __init__(self, ctx: Context, tune: Tuning | None = None, reserve_nodes: int = 0):
+        self.h = ctypes.c_void_p()
+        r = lib().e13_serve_create(ctx.h, ctypes.byref(tune) if tune else None, reserve_nodes, ctypes.byref(self.h))
+        if r:
+            raise E13Error(r, "e13_serve_create")
+
+    def close(self):
+        if self.h:
+            lib().e13_serve_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def clock(self) -> float:
+        return lib().e13_serve_clock(self.h)
+
+    def submit(self, job: Job, job_id: int, t_submit: float = -1.0):
+        r = lib().e13_serve_submit(self.h, ctypes.byref(job), job_id, t_submit)
+        if r:
+            raise E13Error(r, "e13_serve_submit")
+
+    def step(self):
+        res = (ServeResult * 16)()
+        n = ctypes.c_int()
+        r = lib().e13_serve_step(self.h, res, 16, ctypes.byref(n))
+        if r:
+            raise E13Error(r, "e13_serve_step")
+        return [res[i] for i in range(n.value)]
+
+    def pending(self) -> int:
+        return lib().e13_serve_pending(self.h)
+
+    def survivors(self, job_id: int, cap: int = 1 << 16):
+        out = (Survivor * cap)()
+        n = ctypes.c_int()
+        r = lib().e13_serve_survivors(self.h, job_id, out, cap, ctypes.byref(n))
+        if r and r != -7:
+            raise E13Error(r, "e13_serve_survivors")
+        return [out[i] for i in range(min(n.value, cap))]
+
+    def stats(self):
+        ms = ctypes.c_double()
+        ep = ctypes.c_int64()
+        lib().e13_serve_stats(self.h, ctypes.byref(ms), ctypes.byref(ep))
+        return ms.value, ep.value
+
+    def run_all(self, jobs, arrivals=None):
+        """Submits jobs (with optional arrival times) and steps until all are
+        done; returns {id: (ServeResult, [Survivor])}."""
+        for i, job in enumerate(jobs):
+            self.submit(job, i, -1.0 if arrivals is None else arrivals[i])
+        out = {}
+        while self.pending():
+            for r in self.step():
+                out[r.id] = (r, self.survivors(r.id))
+        return out

@@ -162,6 +162,42 @@ void e13_ctx_destroy(e13_ctx *ctx);
 int e13_search(e13_ctx *ctx, const e13_job *job, const e13_tuning *tuning, e13_counts *counts,
                e13_survivor *surv, int surv_cap, int *nsurv);
 
+/* ---- serving: many searches in one persistent kernel ---- */
+
+/* Continuous batching of search jobs (no counterpart in the reference, which
+   runs one search per process).  Up to 16 jobs share the persistent kernel:
+   every node carries its job's slot, and each job has its own counters and
+   survivors.  A job is admitted when a slot is free, its submit time has
+   passed and the frontier stack has room for every running job's reservation
+   (reserve_nodes, 0 = 256 Ki nodes) plus its own.  e13_serve_step admits,
+   runs one epoch (tuning->epoch_us, default 20 ms) and returns the jobs that
+   finished in it: a job is finished when none of its nodes is left on the
+   frontier.  Each job's counts equal those of e13_search on that job alone.
+   A context runs one serve session at a time and no e13_search meanwhile. */
+typedef struct e13_serve e13_serve;
+typedef struct e13_serve_result {
+  int64_t id;
+  int32_t status;            /* E13_OK, or E13_ERR_SURV_CAP if survivor records were lost */
+  int32_t nsurv;             /* survivor records kept for e13_serve_survivors */
+  e13_counts counts;
+  double t_submit, t_start, t_done; /* seconds on the serve clock */
+} e13_serve_result;
+
+int e13_serve_create(e13_ctx *ctx, const e13_tuning *tuning, int64_t reserve_nodes, e13_serve **out);
+void e13_serve_destroy(e13_serve *s);
+/* Seconds since e13_serve_create. */
+double e13_serve_clock(const e13_serve *s);
+/* Queues a job; t_submit < 0 means now (serve clock). */
+int e13_serve_submit(e13_serve *s, const e13_job *job, int64_t id, double t_submit);
+/* One admission + epoch + completion pass; done needs room for 16 results. */
+int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int *ndone);
+/* Jobs queued or running. */
+int64_t e13_serve_pending(const e13_serve *s);
+/* Survivors of a finished job (once; *n = all it found). */
+int e13_serve_survivors(e13_serve *s, int64_t id, e13_survivor *out, int cap, int *n);
+/* CUDA-event time of all epochs and their number. */
+int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs);
+
 /* Autotuner (no counterpart in the reference, which has one fixed GPU
    launch shape): coordinate descent over block size (lanes per CTA), slice
    (steps between refills), warp_stack (subtree depth kept private to a warp
