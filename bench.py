@@ -217,27 +217,37 @@ def main():
     ctx = E.Context(local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
-    kstats = dict(lane_rounds=0.0, warp_rounds=0, donations=0, pool_claims=0, idle_polls=0, epochs=0)
+    kstats = dict(epochs=0, jobs=len(jobs))
 
     def one_step():
+        """One whole search of the workload.  Persistent kernel: all of its jobs
+        (one per deleted state X) run concurrently in one serve session.  Plain
+        kernel: the jobs run one after another, one launch per frontier batch."""
         steps = leaves = 0
         dev_ms = 0.0
         launches = 0
         surv_bytes = 0
-        for job in jobs:
-            c, surv = ctx.search(job, tune)
-            st = ctx.stats()
-            steps += c.steps
-            leaves += c.leaves
-            dev_ms += st.device_ms
-            launches += st.launches
-            surv_bytes += 64 * len(surv)
-            kstats["lane_rounds"] += st.lane_occupancy * st.warp_rounds
-            kstats["warp_rounds"] += st.warp_rounds
-            kstats["donations"] += st.donations
-            kstats["pool_claims"] += st.pool_claims
-            kstats["idle_polls"] += st.idle_polls
-            kstats["epochs"] += st.epochs
+        if kernel == E.KERNEL_PERSISTENT:
+            with E.Server(ctx, E.tuning(epoch_us=200000)) as srv:
+                got = srv.run_all(jobs)
+                ms, epochs = srv.stats()
+            for r, surv in got.values():
+                steps += r.counts.steps
+                leaves += r.counts.leaves
+                surv_bytes += 64 * len(surv)
+            dev_ms = ms
+            launches = 4 * epochs  # search kernel, move, finish, per-job node count
+            kstats["epochs"] += epochs
+        else:
+            for job in jobs:
+                c, surv = ctx.search(job, tune)
+                st = ctx.stats()
+                steps += c.steps
+                leaves += c.leaves
+                dev_ms += st.device_ms
+                launches += st.launches
+                surv_bytes += 64 * len(surv)
+                kstats["epochs"] += st.epochs
         return steps, leaves, dev_ms, launches, surv_bytes
 
     for _ in range(args.warmup):
@@ -282,6 +292,8 @@ def main():
             "scaling": "strong", "vs_baseline": None, "dtype": "int32+u64", "data": "synthetic (reference searches)",
             "leaves_per_s": tot["leaves"] / dev_s, "parity": parity,
             "config": {"workload": f"{args.workload}: {w['desc']}", "kernel": args.kernel,
+                       "jobs": "concurrent in one persistent kernel" if kernel == E.KERNEL_PERSISTENT
+                       else "one after another",
                        "leaves_per_step": w["leaves"], "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"X sharded over {ws} rank(s)"},
             "roofline": {"bound": "int-issue", "achieved": ach_gops, "peak": peak_gops, "unit": "Gop/s",
@@ -292,10 +304,8 @@ def main():
                     "h2d_bytes_per_step": 288 * len(jobs) + 160 * len(jobs),
                     "d2h_bytes_per_step": tot["d2h"] // args.steps + 160 * len(jobs)},
             "gpu_launches": tot["launches"], "clocks": clocks,
-            "kernel_stats": {"lane_occupancy": kstats["lane_rounds"] / max(kstats["warp_rounds"], 1),
-                             "warp_rounds": kstats["warp_rounds"], "donations": kstats["donations"],
-                             "pool_claims": kstats["pool_claims"], "idle_polls": kstats["idle_polls"],
-                             "epochs": kstats["epochs"], "note": "all warmup and timed steps"}}
+            "kernel_stats": {"epochs": kstats["epochs"], "jobs_per_step": kstats["jobs"],
+                             "note": "epochs over all warmup and timed steps"}}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         s, l, dt, kind = run_reference_cpu(WORKLOADS[CPU_SAMPLE], threads)

@@ -160,13 +160,13 @@ void e13_default_tuning(e13_tuning *t) {
   memset(t, 0, sizeof *t);
   t->kernel = E13_KERNEL_PERSISTENT;
   t->block = 768;
-  t->slice = 32;
-  t->warp_stack = 64;
+  t->slice = 16;
+  t->warp_stack = 256;
   t->step_cap = 20000;
   t->batch = 0;
-  t->epoch_us = 500000;
+  t->epoch_us = 200000;
   t->epochs_per_graph = 4;
-  t->pool_low_pct = 25;
+  t->pool_low_pct = 5;
   t->run_skip = 1;
   t->stack_nodes = 0;
 }
