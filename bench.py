@@ -47,7 +47,54 @@ WORKLOADS = {
     "division_v4": dict(desc="freesym erdos_14 9 3 9 F0..I1", machine="erdos_14.txt", mode="freesym", X=[9],
                         free=["F0", "F1", "G0", "G1", "H0", "H1", "I0", "I1"], lo=3, hi=9, leaves=830955779),
 }
+WORKLOADS["serving_mix"] = dict(desc="seeded Poisson stream of 40 search jobs on erdos_14 (seed 2026, 25 jobs/s): "
+                                    "random deleted state, random free set of 2-5 cells (symmetry where setup "
+                                    "allows) or FMAX 2-4, plus counter_sym and FMAX=4 X=11",
+                               machine="erdos_14.txt", mode="mix", X=[], leaves=None)
 CPU_SAMPLE = "local_edits_f3"
+
+
+def serving_mix(seed=2026, n=40, rate=25.0):
+    """The serving-mix job stream: (kind, X, cells, fmax, lo, hi) and arrival times."""
+    import random
+
+    import oracle_lib as O
+
+    rng = random.Random(seed)
+    base = O.load_machine("erdos_14.txt")
+    cells_all = [f"{chr(65 + q)}{a}" for q in range(14) for a in (0, 1)]
+    out, t = [], 0.0
+    while len(out) < n:
+        t += rng.expovariate(rate)
+        X = rng.randrange(14)
+        if len(out) == n // 3:
+            out.append((("free", 13, ["D0", "G0", "K0", "K1", "L1", "M1"], 0, 10, 13), t))  # counter_sym
+            continue
+        if len(out) == 2 * n // 3:
+            out.append((("delete", 11, None, 4, -1, -1), t))
+            continue
+        if rng.random() < 0.5:
+            cells = rng.sample([c for c in cells_all if ord(c[0]) - 65 != X], rng.randint(2, 5))
+            lo = hi = -1
+            if rng.random() < 0.5:
+                lo, hi = sorted(rng.sample(range(1, 14), 2))
+                if not (lo <= X <= hi) or O.setup(base, X, free_cells=cells, lo=lo, hi=hi)[0] < 0:
+                    lo = hi = -1  # symmetry only where setup() accepts it
+            if O.setup(base, X, free_cells=cells, lo=lo, hi=hi)[0] < 0:
+                continue
+            out.append((("free", X, cells, 0, lo, hi), t))
+        else:
+            fmax = rng.randint(2, 4)
+            if fmax == 4 and rng.random() < 0.7:
+                fmax = 3  # keep most jobs small: the stream spans 1e3 .. 1e9 leaves
+            if O.setup(base, X, fmax=fmax)[0] < 0:
+                continue
+            out.append((("delete", X, None, fmax, -1, -1), t))
+    return out
+# DRAM bytes (read + write) of one 200 ms epoch launch of the persistent search
+# kernel, from the ncu capture summarised in
+# profiles/search_kernel_persistent_local_edits_f4.md
+PROFILED_TRAFFIC = {"local_edits_f4": 233.2e6}
 OPS_PER_STEP = 16  # integer lane-ops per simulated step (hash test 2, deadline 1, address 1, load+extract 2,
 #                    index 1, table 2, fork test 1, halt test 1, write test 1, head 2, bounds 2)
 
@@ -180,6 +227,56 @@ def reference_arm(args, w, ws, rank, pg):
         pg.destroy_process_group()
 
 
+def serving_bench(args, w, ws, rank, local, pg):
+    """configs[4] part 1: jobs arrive as a Poisson stream and join the running
+    persistent kernel as slots and frontier memory free up."""
+    import torch
+
+    import e13b200 as E
+    import oracle_lib as O
+
+    base = O.load_machine("erdos_14.txt")
+    stream = serving_mix()
+    jobs, arrivals = [], []
+    for (kind, X, cells, fmax, lo, hi), t in stream:
+        if kind == "free":
+            r, job = E.setup(base, X, free_cells=cells, lo=lo, hi=hi)
+        else:
+            r, job = E.setup(base, X, fmax=fmax)
+        assert r == 0
+        jobs.append(job)
+        arrivals.append(t)
+    ctx = E.Context(local)
+    lat, steps, dev_ms, wall, leaves, epochs = [], 0, 0.0, 0.0, [], 0
+    for it in range(args.warmup + args.steps):
+        with E.Server(ctx) as srv:
+            t0 = time.perf_counter()
+            got = srv.run_all(jobs, arrivals)
+            dt = time.perf_counter() - t0
+            ms, ep = srv.stats()
+        if it >= args.warmup:
+            wall += dt
+            dev_ms += ms
+            epochs += ep
+            for r, surv in got.values():
+                steps += r.counts.steps
+                lat.append(r.t_done - r.t_submit)
+                leaves.append(r.counts.leaves)
+    lat.sort()
+    p = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]
+    line = {"metric": "TM steps/s", "value": steps / wall, "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * wall / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "int32+u64", "data": "synthetic (seeded job stream)",
+            "config": {"workload": f"serving_mix: {w['desc']}", "kernel": "persistent (serve)",
+                       "jobs": len(jobs), "leaves_min": min(leaves), "leaves_max": max(leaves)},
+            "latency_p50_s": p(0.50), "latency_p99_s": p(0.99),
+            "device_busy_frac": dev_ms / 1000 / wall, "gpu_launches": 4 * epochs,
+            "note": "value = steps of all jobs / wall time from the first arrival to the last completion; "
+                    "jobs arrive on the host clock, so idle gaps between arrivals count"}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -201,6 +298,8 @@ def main():
     import oracle_lib as O
 
     torch.cuda.set_device(local)
+    if args.workload == "serving_mix":
+        return serving_bench(args, w, ws, rank, local, pg)
     base = O.load_machine(w["machine"])
     jobs = []
     for X in w["X"]:
@@ -297,7 +396,7 @@ def main():
                        "leaves_per_step": w["leaves"], "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"X sharded over {ws} rank(s)"},
             "roofline": {"bound": "int-issue", "achieved": ach_gops, "peak": peak_gops, "unit": "Gop/s",
-                         "frac": ach_gops / peak_gops, "traffic": None,
+                         "frac": ach_gops / peak_gops, "traffic": PROFILED_TRAFFIC.get(args.workload),
                          "note": f"{OPS_PER_STEP} integer lane-ops per step; peak = {nsm} SMs x 128 lanes x "
                                  f"{sm_mhz:.0f} MHz (median SM clock sampled during the timed region)"},
             "e2e": {"value": tot["steps"] / tot["wall"], "unit": "steps/s",

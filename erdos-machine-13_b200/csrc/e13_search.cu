@@ -1215,8 +1215,9 @@ extern "C" int e13_serve_create(e13_ctx *c, const e13_tuning *tuning, int64_t re
   const long long dump_room = nwarps * (32 + tu.warp_stack);
   s->batch_max = nwarps * 16;
   s->out_nodes = 2 * dump_room + 65536;
-  s->reserve = reserve_nodes > 0 ? reserve_nodes : (1LL << 18);
-  const long long stack_nodes = tu.stack_nodes > 0 ? tu.stack_nodes : (4LL << 20);
+  s->reserve = reserve_nodes > 0 ? reserve_nodes : (1LL << 16);
+  // serving keeps many frontiers resident: 16 Mi nodes (5 GB) by default
+  const long long stack_nodes = tu.stack_nodes > 0 ? tu.stack_nodes : (16LL << 20);
   if ((rc = grow(&c->stack, &c->stack_cap, stack_nodes))) return rc;
   if ((rc = grow(&c->out, &c->out_cap, s->out_nodes))) return rc;
   if ((rc = grow(&c->wstack, &c->wstack_nodes, nwarps * tu.warp_stack))) return rc;

@@ -169,7 +169,8 @@ int e13_search(e13_ctx *ctx, const e13_job *job, const e13_tuning *tuning, e13_c
    every node carries its job's slot, and each job has its own counters and
    survivors.  A job is admitted when a slot is free, its submit time has
    passed and the frontier stack has room for every running job's reservation
-   (reserve_nodes, 0 = 256 Ki nodes) plus its own.  e13_serve_step admits,
+   (reserve_nodes, 0 = 64 Ki nodes) plus its own; the serve stack holds
+   tuning->stack_nodes nodes (0 = 16 Mi nodes, 5 GB).  e13_serve_step admits,
    runs one epoch (tuning->epoch_us, default 20 ms) and returns the jobs that
    finished in it: a job is finished when none of its nodes is left on the
    frontier.  Each job's counts equal those of e13_search on that job alone.

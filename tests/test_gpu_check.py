@@ -67,3 +67,19 @@ def test_deep15_v1_sample():
     # the golden file was made in chunks whose ids restart: compare the text after the id
     for i, ci, o in zip(idx, ins, outs):
         assert E.format_deep(ci, o, 15) == exp[i].split(" ", 2)[2]
+
+
+def test_search_feeds_device_recheck(searches):
+    """The pipeline of the division and counter searches: survivors of a device
+    search go straight to the device recheck.  The 61 counter survivors are all
+    consistent to stage 15 (recheck.c on the reference's survivors says the
+    same); the lines equal the golden survivors, so the verdicts are theirs."""
+    from gpu_common import make_job
+    e = searches["counter_sym"]
+    job = make_job(e, 13)
+    c, surv = ctx().search(job)
+    lines = [E.survivor_line(job, s) for s in surv]
+    assert len(lines) == 61
+    outs = ctx().check([E.parse_survivor_line(l) for l in lines], 15, 0)
+    verdicts = [E.format_recheck(o, 15) for o in outs]
+    assert all(v.startswith("CONSISTENT to n=15") for v in verdicts), verdicts[:3]
