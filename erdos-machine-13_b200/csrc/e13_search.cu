@@ -37,9 +37,9 @@ using namespace e13dev;
 namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
-constexpr int kMaxBlock = 896;
 constexpr int kKeySmemBytes = (kTapeCells + 64) * 8;
 constexpr long long kPoolNodes = 1LL << 18;  // donation pool: 256 Ki nodes (80 MiB)
+constexpr long long kWholeFrontier = 1LL << 62;  // persistent batch when e13_tuning::batch is 0
 
 // steps a lane gets between warp-level refill rounds is Params::slice
 
@@ -161,11 +161,6 @@ __device__ __forceinline__ void record_survivor(const Params &P, const Lane &L, 
 }
 
 enum { kStRun = 0, kStIdle = 1, kStFork = 2, kStCap = 3 };
-
-__device__ __forceinline__ void copy_node_cg(Node *dst, const Node *src, int lane) {
-  // a pool node written by another SM: read past L1
-  if (lane < kNodeChunks) reinterpret_cast<uint4 *>(dst)[lane] = __ldcg(reinterpret_cast<const uint4 *>(src) + lane);
-}
 
 __device__ __forceinline__ int wrap(int s, int d) { return s >= d ? s - d : s; }
 
@@ -922,7 +917,9 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   const long long dump_room = nwarps * (32 + (persist ? tu.warp_stack : 0));
   long long out_nodes, batch_max;
   if (persist) {
-    batch_max = tu.batch > 0 ? tu.batch : nwarps * 16;
+    // every epoch may take the whole frontier: an epoch then ends on its time
+    // bound, not in a tail where a few warps finish the last input subtrees
+    batch_max = tu.batch > 0 ? tu.batch : kWholeFrontier;
     out_nodes = 2 * dump_room + 65536;
   } else {
     batch_max = tu.batch > 0 ? tu.batch : 16384;
@@ -1120,7 +1117,8 @@ extern "C" int e13_autotune(e13_ctx *c, const e13_job *job, const e13_tuning *st
   const Axis axes[] = {
       {&e13_tuning::block, {512, 640, 768, 0}, 3},
       {&e13_tuning::slice, {16, 32, 64, 128}, 4},
-      {&e13_tuning::warp_stack, {16, 32, 64, 128}, 4},
+      {&e13_tuning::warp_stack, {64, 128, 256, 512}, 4},
+      {&e13_tuning::batch, {0, 65536, 1 << 20, 0}, 3},
       {&e13_tuning::pool_low_pct, {5, 12, 25, 50}, 4},
   };
   for (const Axis &ax : axes) {
@@ -1200,6 +1198,7 @@ extern "C" int e13_serve_create(e13_ctx *c, const e13_tuning *tuning, int64_t re
     if (tuning->warp_stack) tu.warp_stack = tuning->warp_stack;
     if (tuning->epoch_us) tu.epoch_us = tuning->epoch_us;
     if (tuning->pool_low_pct) tu.pool_low_pct = tuning->pool_low_pct;
+    if (tuning->batch) tu.batch = tuning->batch;
     tu.run_skip = tuning->run_skip;
     if (tuning->stack_nodes) tu.stack_nodes = tuning->stack_nodes;
   }
@@ -1213,7 +1212,7 @@ extern "C" int e13_serve_create(e13_ctx *c, const e13_tuning *tuning, int64_t re
   s->tu = tu;
   const long long nwarps = (long long)c->nsm * tu.block / 32;
   const long long dump_room = nwarps * (32 + tu.warp_stack);
-  s->batch_max = nwarps * 16;
+  s->batch_max = tu.batch > 0 ? tu.batch : kWholeFrontier;
   s->out_nodes = 2 * dump_room + 65536;
   s->reserve = reserve_nodes > 0 ? reserve_nodes : (1LL << 16);
   // serving keeps many frontiers resident: 16 Mi nodes (5 GB) by default

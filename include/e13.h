@@ -88,7 +88,8 @@ typedef struct e13_tuning {
   int32_t slice;             /* steps per round between warp-level refills */
   int32_t warp_stack;        /* nodes in each warp's private DFS stack (persistent) */
   int32_t step_cap;          /* plain kernel: steps per work item before it is requeued */
-  int32_t batch;             /* nodes taken from the frontier per launch / epoch (0 = auto) */
+  int32_t batch;             /* nodes taken from the frontier per launch / epoch (0 = auto: the whole
+                                frontier for the persistent kernel, 16384 for the plain one) */
   int32_t epoch_us;          /* persistent: wall-clock bound of one epoch, microseconds */
   int32_t epochs_per_graph;  /* persistent: epochs captured in one CUDA graph */
   int32_t pool_low_pct;      /* persistent: warps donate stack nodes while the pool holds fewer than this % of warps */
