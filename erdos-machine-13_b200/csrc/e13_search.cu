@@ -205,6 +205,17 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   Lane L;
   L.t = 0;
   L.tseg = 0;
+  // leaves and steps of this lane's current job, added to the block's per-job
+  // counters only when the lane changes job and at the end (no atomics per leaf)
+  u32 acc_leaves = 0, acc_steps = 0;
+  auto flush_counts = [&]() {
+    if (acc_leaves | acc_steps) {
+      atomicAdd(&s_jc[L.job][0], (unsigned long long)acc_leaves);
+      atomicAdd(&s_jc[L.job][1], (unsigned long long)acc_steps);
+      acc_leaves = 0;
+      acc_steps = 0;
+    }
+  };
   int status = kStIdle;
   int fork_cell = 0;
   u32 fork_e = 0;
@@ -415,6 +426,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
       if (status == kStIdle && rank < navail) {
         int ch = -1;
         if (!(cur_keep && rank == 0)) ch = nth_bit64(cur_vm, rank - cur_keep);
+        if (N->job != L.job) flush_counts();
         lane_load(L, N, tcol, rcol, stride, P.nq);
         apply_child(L, N, ch, rcol, stride, s_jp[N->job].y, s_jp[N->job].z, P.run_skip);
         status = kStRun;
@@ -469,7 +481,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
       if (d && rounds > 0) {
         // dump: live lanes as resume nodes, then this warp's stack
         if (status == kStRun) {
-          atomicAdd(&s_jc[L.job][1], (unsigned long long)(L.t - L.tseg));
+          acc_steps += (u32)(L.t - L.tseg);
           L.tseg = L.t;
           const unsigned long long k = atomicAdd(&ctl->nout, 1ull);
           if ((long long)k < P.out_cap) lane_store(L, P.out + k, tcol, rcol, stride, P.nq, -1, 1, 0ull);
@@ -537,9 +549,13 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
               if (e == kEntHalt) {
                 ev = kEvDead;
               } else if (e == kEntFree || L.budget > 0) {
-                // a fork: handled by the warp at the next round
-                atomicAdd(&s_jc[L.job][1], (unsigned long long)(L.t - L.tseg));
-                L.tseg = L.t;
+                // a fork: handled by the warp at the next round (the persistent
+                // kernel goes on with the first child in this lane, so its
+                // steps are counted at the leaf)
+                if (!PERSIST) {
+                  acc_steps += (u32)(L.t - L.tseg);
+                  L.tseg = L.t;
+                }
                 fork_cell = cell;
                 fork_e = e;
                 status = kStFork;
@@ -552,9 +568,10 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
             }
             if (ev) {
               // a leaf
-              atomicAdd(&s_jc[L.job][1], (unsigned long long)(L.t - L.tseg));
+              acc_steps += (u32)(L.t - L.tseg);
               L.tseg = L.t;
-              atomicAdd(&s_jc[L.job][0], 1ull);
+              ++acc_leaves;
+              if (acc_steps >= 0x80000000u) flush_counts();
               if (ev == kEvDead) atomicAdd(&s_jc[L.job][2 + L.stage], 1ull);
               else record_survivor(P, L, rcol, stride);
               status = kStIdle;
@@ -566,8 +583,9 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
           __syncwarp();
         }
         if (!PERSIST && status == kStRun && L.t - L.tseg >= P.step_cap) {
-          atomicAdd(&s_jc[L.job][1], (unsigned long long)(L.t - L.tseg));
+          acc_steps += (u32)(L.t - L.tseg);
           L.tseg = L.t;
+          if (acc_steps >= 0x80000000u) flush_counts();
           status = kStCap;
         }
       }
@@ -575,6 +593,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   }
 
   // ---- totals
+  flush_counts();
   if (lane == 0) {
     atomicAdd(&ctl->rounds, (unsigned long long)rounds);
     atomicAdd(&ctl->lane_rounds, st_lane_rounds);
