@@ -16,9 +16,9 @@ simulated Turing-machine steps per second (leaves/s is reported beside it).
             bounded sample: the FMAX = 3 local-edit search
 
 --impl reference runs that reference CPU program instead (the reference arm).
-Under torchrun (N > 1) each rank runs the X values X = rank mod N (the search
-splits into independent per-X jobs; totals are summed, the time is the max
-over ranks).
+Under torchrun (N > 1) rank r runs every N-th X starting at r (the search
+splits into independent per-X jobs; e13shard.py sums the totals and takes the
+maximum of the times over ranks).
 """
 from __future__ import annotations
 
@@ -300,11 +300,11 @@ def main():
     torch.cuda.set_device(local)
     if args.workload == "serving_mix":
         return serving_bench(args, w, ws, rank, local, pg)
+    import e13shard as S
+
     base = O.load_machine(w["machine"])
     jobs = []
-    for X in w["X"]:
-        if X % ws != rank:
-            continue
+    for X in S.share(w["X"], rank, ws):
         if w["mode"] == "delete":
             r, job = E.setup(base, X, fmax=w["fmax"])
         else:
@@ -373,12 +373,10 @@ def main():
         pg.barrier()
     clocks = sampler.summary()
     if pg:
-        t = torch.tensor([tot["dev_ms"], tot["wall"]], dtype=torch.float64, device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        c = torch.tensor([tot["steps"], tot["leaves"], tot["launches"]], dtype=torch.float64, device=f"cuda:{local}")
-        pg.all_reduce(c)
-        tot["dev_ms"], tot["wall"] = float(t[0]), float(t[1])
-        tot["steps"], tot["leaves"], tot["launches"] = int(c[0]), int(c[1]), int(c[2])
+        sums, maxes = S.reduce_totals(pg, {k: tot[k] for k in ("steps", "leaves", "launches", "d2h")},
+                                      {k: tot[k] for k in ("dev_ms", "wall")}, device=f"cuda:{local}")
+        tot.update(sums)
+        tot.update(maxes)
     parity = tot["leaves"] == w["leaves"] * args.steps
     dev_s = tot["dev_ms"] / 1000.0
     value = tot["steps"] / dev_s
