@@ -9,7 +9,12 @@
 
    Survivors go to stdout in the reference's format, one summary line per X to
    stderr.  Environment: E13_DEVICE (CUDA device, default 0), E13_KERNEL
-   (persistent | plain).  There is no CPU path: without a GPU it exits 1. */
+   (persistent | plain).  There is no CPU path: without a GPU it exits 1.
+
+   free / freesym keep checkpoints as src/e13gpu.py:349-409 does: E13_CKPT
+   names the checkpoint (resumed when it exists), E13_CKPT_SEC the seconds
+   between saves (default 1800), and creating <E13_CKPT>.stop stops the run
+   cleanly with a checkpoint and exit status 3; the same command resumes it. */
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -34,14 +39,34 @@ static e13_ctx *open_ctx(void) {
   return ctx;
 }
 
-static int run_one(e13_ctx *ctx, const e13_job *job, const e13_tuning *tu) {
+/* ck: NULL, or the checkpoint of a free / freesym run */
+static int run_one(e13_ctx *ctx, const e13_job *job, const e13_tuning *tu, const e13_checkpoint *ck) {
   int cap = 1 << 16;
   e13_survivor *surv = (e13_survivor *)malloc(sizeof(e13_survivor) * (size_t)cap);
   e13_counts c;
   int ns = 0;
-  double w0 = now_s();
-  int rc = e13_search(ctx, job, tu, &c, surv, cap, &ns);
-  double wall = now_s() - w0;
+  double w0 = now_s(), wall = 0.0;
+  int rc;
+  if (ck) {
+    FILE *pf = fopen(ck->path, "r");
+    if (pf) {
+      char slot[4] = {0};
+      if (fgets(slot, sizeof slot, pf)) fprintf(stderr, "resuming from %s.%c\n", ck->path, slot[0]);
+      fclose(pf);
+    }
+    int64_t left = 0;
+    rc = e13_search_resumable(ctx, job, tu, ck, &c, surv, cap, &ns, &wall, &left);
+    if (rc == E13_STOPPED) {
+      fprintf(stderr, "STOPPED cleanly at wall=%.0fs steps=%.3e survivors=%d stack=%lld; run the same command to "
+              "resume\n", wall, (double)c.steps, ns, (long long)left);
+      free(surv);
+      return E13_STOPPED;
+    }
+    if (rc == E13_ERR_CKPT) fprintf(stderr, "checkpoint %s is unreadable or for another run\n", ck->path);
+  } else {
+    rc = e13_search(ctx, job, tu, &c, surv, cap, &ns);
+    wall = now_s() - w0;
+  }
   if (rc && rc != E13_ERR_SURV_CAP) {
     fprintf(stderr, "X=%d search failed (error %d)\n", job->X, rc);
     free(surv);
@@ -128,7 +153,7 @@ int main(int argc, char **argv) {
         fprintf(stderr, "X=%d: setup error %d\n", X, rc);
         return 1;
       }
-      if (run_one(ctx, &job, &tu)) return 1;
+      if (run_one(ctx, &job, &tu, NULL)) return 1;
     }
     e13_ctx_destroy(ctx);
     return 0;
@@ -161,10 +186,18 @@ int main(int argc, char **argv) {
       fprintf(stderr, "setup error %d\n", rc);
       return 1;
     }
+    /* the run's identity for its checkpoint: mode, arguments and machine file name */
+    char config[1024];
+    const char *slash = strrchr(argv[2], '/');
+    int n = snprintf(config, sizeof config, "%s %s", mode, slash ? slash + 1 : argv[2]);
+    for (int i = 3; i < argc && n < (int)sizeof config; i++) n += snprintf(config + n, sizeof config - n, " %s", argv[i]);
+    const char *ckpath = getenv("E13_CKPT");
+    const char *cksec = getenv("E13_CKPT_SEC");
+    e13_checkpoint ck = {ckpath, config, cksec ? atof(cksec) : 1800.0, 0.0};
     e13_ctx *ctx = open_ctx();
-    rc = run_one(ctx, &job, &tu);
+    rc = run_one(ctx, &job, &tu, (ckpath && ckpath[0]) ? &ck : NULL);
     e13_ctx_destroy(ctx);
-    return rc ? 1 : 0;
+    return rc == E13_STOPPED ? 3 : (rc ? 1 : 0);
   }
   fprintf(stderr, "unknown mode %s\n", mode);
   return 1;

@@ -25,8 +25,12 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
+#include <chrono>
+#include <string>
 #include <vector>
 
 #include "e13.h"
@@ -900,8 +904,210 @@ static void decode_survivor(const SurvRec &r, int nq, e13_survivor *s) {
   s->steps = r.t;
 }
 
-extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuning, e13_counts *counts,
-                          e13_survivor *surv, int surv_cap, int *nsurv) {
+// ------------------------------------------------------------------------
+// checkpoint files of one search (e13_search_resumable)
+//
+// <path>.<slot>.bin   the frontier stack: top nodes as they are on the device
+// <path>.<slot>.meta  CkptHeader, the config string, the job's counters, the
+//                     survivor records
+// <path>              the slot of the last complete checkpoint ("a" or "b")
+
+namespace {
+
+constexpr char kCkptMagic[8] = {'E', '1', '3', 'C', 'K', 'P', 'T', '1'};
+constexpr long long kCkptChunk = 1LL << 16;  // nodes per host transfer (20 MiB)
+
+struct CkptHeader {
+  char magic[8];
+  uint32_t node_bytes, job_counters, surv_bytes, config_len;
+  int64_t top, peak, launches;
+  double wall;  // seconds of the search before this checkpoint
+  uint64_t nsurv, nrec;
+  e13_job job;
+};
+
+double host_seconds() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+bool file_exists(const std::string &path) {
+  struct stat st;
+  return stat(path.c_str(), &st) == 0;
+}
+
+std::string slot_file(const e13_checkpoint *ck, int slot, const char *ext) {
+  return std::string(ck->path) + (slot ? ".b" : ".a") + ext;
+}
+
+bool write_all(FILE *f, const void *p, size_t n) { return n == 0 || fwrite(p, 1, n, f) == n; }
+bool read_all(FILE *f, void *p, size_t n) { return n == 0 || fread(p, 1, n, f) == n; }
+
+// flush, fsync and close: true only if the data reached the disk
+bool close_synced(FILE *f) {
+  const bool ok = fflush(f) == 0 && fsync(fileno(f)) == 0;
+  return fclose(f) == 0 && ok;
+}
+
+// Writes the state after the last epoch (ctl_host is current) to `slot`, then
+// points the pointer file at it.
+int ckpt_save(e13_ctx *c, const e13_job *job, const e13_checkpoint *ck, int slot, double wall) {
+  const Ctl &h = *c->ctl_host;
+  const long long top = h.top;
+  FILE *f = fopen(slot_file(ck, slot, ".bin").c_str(), "wb");
+  if (!f) return E13_ERR_IO;
+  std::vector<Node> buf((size_t)std::min(std::max(top, 1LL), kCkptChunk));
+  for (long long o = 0; o < top; o += kCkptChunk) {
+    const long long n = std::min(kCkptChunk, top - o);
+    if (cudaMemcpyAsync(buf.data(), c->stack + o, sizeof(Node) * n, cudaMemcpyDeviceToHost, c->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess) {
+      fclose(f);
+      return E13_ERR_CUDA;
+    }
+    if (!write_all(f, buf.data(), sizeof(Node) * (size_t)n)) {
+      fclose(f);
+      return E13_ERR_IO;
+    }
+  }
+  if (!close_synced(f)) return E13_ERR_IO;
+
+  unsigned long long cnt[kJobCounters];
+  const unsigned long long nrec = std::min<unsigned long long>(h.nsurv, (unsigned long long)c->surv_cap);
+  std::vector<SurvRec> recs((size_t)nrec);
+  CK(cudaMemcpyAsync(cnt, c->d_jobcnt, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
+  if (nrec) CK(cudaMemcpyAsync(recs.data(), c->surv, sizeof(SurvRec) * nrec, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  CkptHeader hd;
+  memset(&hd, 0, sizeof hd);
+  memcpy(hd.magic, kCkptMagic, sizeof hd.magic);
+  hd.node_bytes = sizeof(Node);
+  hd.job_counters = kJobCounters;
+  hd.surv_bytes = sizeof(SurvRec);
+  hd.config_len = (uint32_t)strlen(ck->config);
+  hd.top = top;
+  hd.peak = h.peak;
+  hd.launches = h.launches;
+  hd.wall = wall;
+  hd.nsurv = h.nsurv;
+  hd.nrec = nrec;
+  hd.job = *job;
+  f = fopen(slot_file(ck, slot, ".meta").c_str(), "wb");
+  if (!f) return E13_ERR_IO;
+  const bool ok = write_all(f, &hd, sizeof hd) && write_all(f, ck->config, hd.config_len) &&
+                  write_all(f, cnt, sizeof cnt) && write_all(f, recs.data(), sizeof(SurvRec) * (size_t)nrec);
+  if (!close_synced(f) || !ok) return E13_ERR_IO;
+
+  // the pointer last: until the rename the previous checkpoint stays the valid one
+  const std::string tmp = std::string(ck->path) + ".tmp";
+  f = fopen(tmp.c_str(), "wb");
+  if (!f) return E13_ERR_IO;
+  const bool pok = write_all(f, slot ? "b\n" : "a\n", 2);
+  if (!close_synced(f) || !pok || rename(tmp.c_str(), ck->path) != 0) return E13_ERR_IO;
+  return E13_OK;
+}
+
+// Loads the slot the pointer file names onto the device (stack, control
+// block, counters, survivors).  *slot = the slot read.
+int ckpt_load(e13_ctx *c, const e13_job *job, const e13_checkpoint *ck, long long batch_max, long long room,
+              int *slot, double *prior_wall) {
+  FILE *f = fopen(ck->path, "rb");
+  if (!f) return E13_ERR_CKPT;
+  char name[4] = {0};
+  const size_t got = fread(name, 1, 3, f);
+  fclose(f);
+  if (got < 1 || (name[0] != 'a' && name[0] != 'b')) return E13_ERR_CKPT;
+  *slot = name[0] == 'b';
+
+  f = fopen(slot_file(ck, *slot, ".meta").c_str(), "rb");
+  if (!f) return E13_ERR_CKPT;
+  CkptHeader hd;
+  std::string cfg;
+  unsigned long long cnt[kJobCounters];
+  bool ok = read_all(f, &hd, sizeof hd) && !memcmp(hd.magic, kCkptMagic, sizeof hd.magic) &&
+            hd.node_bytes == sizeof(Node) && hd.job_counters == kJobCounters && hd.surv_bytes == sizeof(SurvRec) &&
+            hd.config_len == strlen(ck->config) && hd.top >= 0 && hd.nrec <= hd.nsurv;
+  if (ok) {
+    cfg.resize(hd.config_len);
+    ok = read_all(f, &cfg[0], hd.config_len) && cfg == ck->config && !memcmp(&hd.job, job, sizeof *job) &&
+         read_all(f, cnt, sizeof cnt);
+  }
+  std::vector<SurvRec> recs;
+  if (ok) {
+    recs.resize((size_t)hd.nrec);
+    ok = read_all(f, recs.data(), sizeof(SurvRec) * (size_t)hd.nrec);
+  }
+  fclose(f);
+  if (!ok) return E13_ERR_CKPT;
+  if (hd.top > room) return E13_ERR_OVERFLOW;
+
+  const std::string bin = slot_file(ck, *slot, ".bin");
+  struct stat st;
+  if (stat(bin.c_str(), &st) != 0 || (long long)st.st_size != hd.top * (long long)sizeof(Node)) return E13_ERR_CKPT;
+  f = fopen(bin.c_str(), "rb");
+  if (!f) return E13_ERR_CKPT;
+  std::vector<Node> buf((size_t)std::min(std::max((long long)hd.top, 1LL), kCkptChunk));
+  for (long long o = 0; o < hd.top; o += kCkptChunk) {
+    const long long n = std::min(kCkptChunk, (long long)hd.top - o);
+    if (!read_all(f, buf.data(), sizeof(Node) * (size_t)n)) {
+      fclose(f);
+      return E13_ERR_CKPT;
+    }
+    if (cudaMemcpyAsync(c->stack + o, buf.data(), sizeof(Node) * n, cudaMemcpyHostToDevice, c->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess) {
+      fclose(f);
+      return E13_ERR_CUDA;
+    }
+  }
+  fclose(f);
+
+  int rc;
+  if ((rc = grow(&c->surv, &c->surv_cap, std::max<long long>((long long)hd.nrec, c->surv_cap)))) return rc;
+  memset(c->ctl_host, 0, sizeof(Ctl));
+  c->ctl_host->top = hd.top;
+  c->ctl_host->batch = std::min<long long>(hd.top, batch_max);
+  c->ctl_host->peak = std::max<long long>(hd.peak, hd.top);
+  c->ctl_host->launches = (int)hd.launches;
+  c->ctl_host->nsurv = hd.nsurv;
+  CK(cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_jobcnt, cnt, sizeof cnt, cudaMemcpyHostToDevice, c->stream));
+  if (hd.nrec) CK(cudaMemcpyAsync(c->surv, recs.data(), sizeof(SurvRec) * hd.nrec, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *prior_wall = hd.wall;
+  return E13_OK;
+}
+
+void ckpt_remove(const e13_checkpoint *ck) {
+  remove(ck->path);
+  for (int slot = 0; slot < 2; ++slot) {
+    remove(slot_file(ck, slot, ".bin").c_str());
+    remove(slot_file(ck, slot, ".meta").c_str());
+  }
+  remove((std::string(ck->path) + ".tmp").c_str());
+}
+
+// Whether to checkpoint now: 0 no, 1 save, 2 save and stop.
+struct CkptClock {
+  const e13_checkpoint *ck;
+  std::string stop_file;
+  double t_call, last_save, last_look;
+  int due(double now) {
+    if (ck->stop_after_s > 0 && now - t_call >= ck->stop_after_s) return 2;
+    if (now - last_look >= 1.0) {
+      last_look = now;
+      if (file_exists(stop_file)) return 2;
+    }
+    const double every = ck->interval_s > 0 ? ck->interval_s : 1800.0;
+    return now - last_save >= every ? 1 : 0;
+  }
+};
+
+}  // namespace
+
+static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning, const e13_checkpoint *ck,
+                       e13_counts *counts, e13_survivor *surv, int surv_cap, int *nsurv, double *wall_s,
+                       int64_t *frontier) {
+  const double t_call = host_seconds();
   if (!c || !job || !counts || !nsurv || (surv_cap > 0 && !surv) || surv_cap < 0) return E13_ERR_ARG;
   if (job->nq < 1 || job->nq > 16) return E13_ERR_NQ;
   if (job->budget < 0) return E13_ERR_FMAX;
@@ -996,6 +1202,36 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
   // pool slots carry the tag of the launch that wrote them; tags restart with every search
   if (persist) CK(cudaMemsetAsync(c->pool_ready, 0, sizeof(int) * (size_t)c->pool_ready_cap, c->stream));
   CK(cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+
+  // checkpoints: resume from the last complete slot, then save into the other one
+  double prior_wall = 0.0;
+  int slot = 0;
+  bool stopped = false;
+  CkptClock clk{ck, ck ? std::string(ck->path) + ".stop" : std::string(), t_call, t_call, t_call};
+  if (ck) {
+    if (file_exists(clk.stop_file)) remove(clk.stop_file.c_str());  // left from the last clean stop
+    if (file_exists(ck->path)) {
+      int loaded = 0;
+      if ((rc = ckpt_load(c, job, ck, batch_max, c->stack_cap - out_nodes, &loaded, &prior_wall))) return rc;
+      slot = loaded ^ 1;
+    }
+  }
+  auto checkpoint_step = [&](int &status) -> bool {  // true: leave the launch loop
+    if (!ck || c->ctl_host->top == 0) return false;
+    const double now = host_seconds();
+    const int act = clk.due(now);
+    if (!act) return false;
+    const int r = ckpt_save(c, job, ck, slot, prior_wall + (now - t_call));
+    if (r) {
+      status = r;
+      return true;
+    }
+    slot ^= 1;
+    clk.last_save = host_seconds();
+    stopped = act == 2;
+    if (stopped && file_exists(clk.stop_file)) remove(clk.stop_file.c_str());  // consumed by this stop
+    return stopped;
+  };
   CK(cudaEventRecord(c->ev0, c->stream));
 
   const int move_blocks = c->nsm * 4;
@@ -1027,6 +1263,7 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
         break;
       }
       if (c->ctl_host->top == 0) break;
+      if (checkpoint_step(err)) break;
     }
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
@@ -1049,6 +1286,7 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
         break;
       }
       if (c->ctl_host->top == 0) break;
+      if (checkpoint_step(err)) break;
     }
   }
   CK(cudaEventRecord(c->ev1, c->stream));
@@ -1084,8 +1322,24 @@ extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuni
     CK(cudaMemcpy(recs.data(), c->surv, sizeof(SurvRec) * (size_t)ncopy, cudaMemcpyDeviceToHost));
     for (long long i = 0; i < ncopy; ++i) decode_survivor(recs[(size_t)i], job->nq, &surv[i]);
   }
+  if (wall_s) *wall_s = prior_wall + (host_seconds() - t_call);
+  if (frontier) *frontier = stopped ? h.top : 0;
+  if (stopped) return E13_STOPPED;
+  if (ck) ckpt_remove(ck);
   if (ns > surv_cap || ns > c->surv_cap) return E13_ERR_SURV_CAP;
   return E13_OK;
+}
+
+extern "C" int e13_search(e13_ctx *c, const e13_job *job, const e13_tuning *tuning, e13_counts *counts,
+                          e13_survivor *surv, int surv_cap, int *nsurv) {
+  return search_impl(c, job, tuning, nullptr, counts, surv, surv_cap, nsurv, nullptr, nullptr);
+}
+
+extern "C" int e13_search_resumable(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
+                                    const e13_checkpoint *ck, e13_counts *counts, e13_survivor *surv, int surv_cap,
+                                    int *nsurv, double *wall_s, int64_t *frontier) {
+  if (!ck || !ck->path || !ck->config || !ck->path[0]) return E13_ERR_ARG;
+  return search_impl(c, job, tuning, ck, counts, surv, surv_cap, nsurv, wall_s, frontier);
 }
 
 extern "C" int e13_run_full(e13_ctx *c, const int32_t *tabs, int n, int nq, int64_t *out) {

@@ -27,7 +27,9 @@ ERRORS = {
     -4: "start state in the symmetric states", -5: "CUDA error", -6: "frontier stack overflow",
     -7: "survivor buffer too small", -8: "too many states", -9: "cannot open machine file",
     -10: "device wait timed out", -11: "no CUDA device", -12: "more than the fixed no-allocation memory holds",
+    -13: "checkpoint unreadable or of another run",
 }
+STOPPED = 3  # e13_search_resumable stopped cleanly with a checkpoint
 E13_CHECK_NOALLOC_MAX = 16
 
 
@@ -35,6 +37,11 @@ class E13Error(RuntimeError):
     def __init__(self, code, what=""):
         super().__init__(f"{what}: {ERRORS.get(code, code)} ({code})")
         self.code = code
+
+
+class Checkpoint(ctypes.Structure):
+    _fields_ = [("path", ctypes.c_char_p), ("config", ctypes.c_char_p), ("interval_s", ctypes.c_double),
+                ("stop_after_s", ctypes.c_double)]
 
 
 class Job(ctypes.Structure):
@@ -128,6 +135,8 @@ def lib():
         L.e13_ctx_destroy.argtypes = [ctypes.c_void_p]
         L.e13_ctx_destroy.restype = None
         L.e13_search.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Counts), P(Survivor), I, P(I)]
+        L.e13_search_resumable.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Checkpoint), P(Counts),
+                                           P(Survivor), I, P(I), P(ctypes.c_double), P(ctypes.c_int64)]
         L.e13_last_stats.argtypes = [ctypes.c_void_p, P(Stats)]
         L.e13_autotune.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Tuning), P(ctypes.c_double)]
         L.e13_serve_create.argtypes = [ctypes.c_void_p, P(Tuning), ctypes.c_int64, P(ctypes.c_void_p)]
@@ -155,7 +164,7 @@ def lib():
 
 EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine", "e13_setup",
             "e13_format_survivor", "e13_format_summary", "e13_default_tuning", "e13_ctx_create", "e13_ctx_destroy",
-            "e13_search", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
+            "e13_search", "e13_search_resumable", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
             "e13_format_recheck", "e13_format_deep", "e13_raw_run", "e13_autotune", "e13_check_noalloc",
             "e13_serve_create", "e13_serve_destroy", "e13_serve_clock", "e13_serve_submit", "e13_serve_step",
             "e13_serve_pending", "e13_serve_survivors", "e13_serve_stats"]
@@ -238,6 +247,24 @@ class Context:
         if r and r != -7:
             raise E13Error(r, "e13_search")
         return counts, [surv[i] for i in range(min(ns.value, surv_cap))]
+
+    def search_resumable(self, job: Job, path: str, config: str, interval_s: float = 0.0,
+                         stop_after_s: float = 0.0, tune: Tuning | None = None, surv_cap: int = 1 << 16):
+        """e13_search with checkpoints at `path`.  Returns (status, counts,
+        survivors, wall seconds over all calls, frontier nodes left); status is
+        0 when the search finished, STOPPED when it stopped with a checkpoint."""
+        ck = Checkpoint(path.encode(), config.encode(), interval_s, stop_after_s)
+        counts = Counts()
+        surv = (Survivor * max(surv_cap, 1))()
+        ns = ctypes.c_int()
+        wall = ctypes.c_double()
+        left = ctypes.c_int64()
+        r = lib().e13_search_resumable(self.h, ctypes.byref(job), ctypes.byref(tune) if tune else None,
+                                       ctypes.byref(ck), ctypes.byref(counts), surv, surv_cap, ctypes.byref(ns),
+                                       ctypes.byref(wall), ctypes.byref(left))
+        if r not in (0, -7, STOPPED):
+            raise E13Error(r, "e13_search_resumable")
+        return r, counts, [surv[i] for i in range(min(ns.value, surv_cap))], wall.value, left.value
 
     def autotune(self, job: Job, start: Tuning | None = None):
         """Coordinate-descent tuning of the persistent kernel on `job`; returns (Tuning, best ms)."""

@@ -43,7 +43,9 @@ enum {
   E13_ERR_IO = -9,           /* machine file missing or unreadable (src/e13search.c:113) */
   E13_ERR_TIMEOUT = -10,     /* a device wait ran out (bounded waits; no hang) */
   E13_ERR_NO_DEVICE = -11,   /* no CUDA device: there is no CPU fallback */
-  E13_ERR_NOALLOC_SIZE = -12 /* e13_check_noalloc: more machines (or a larger nmax) than its fixed memory holds */
+  E13_ERR_NOALLOC_SIZE = -12, /* e13_check_noalloc: more machines (or a larger nmax) than its fixed memory holds */
+  E13_ERR_CKPT = -13,        /* checkpoint unreadable, truncated, or of another run or job */
+  E13_STOPPED = 3            /* e13_search_resumable: stopped cleanly, checkpoint written (not an error) */
 };
 
 /* A prepared candidate family: base machine with state X deleted.
@@ -162,6 +164,35 @@ void e13_ctx_destroy(e13_ctx *ctx);
    in the reference (src/e13search.c:185): compare sorted lines. */
 int e13_search(e13_ctx *ctx, const e13_job *job, const e13_tuning *tuning, e13_counts *counts,
                e13_survivor *surv, int surv_cap, int *nsurv);
+
+/* ---- checkpoint / resume of one search ---- */
+
+typedef struct e13_checkpoint {
+  const char *path;     /* pointer file: names the last complete slot, "a" or "b"; the slots are
+                           <path>.a.bin + <path>.a.meta and <path>.b.bin + <path>.b.meta */
+  const char *config;   /* identity of the run (the CLI passes its arguments); a checkpoint written
+                           under another config, job or node format is refused: E13_ERR_CKPT */
+  double interval_s;    /* seconds between checkpoints; <= 0: 1800 (the reference's E13_CKPT_SEC) */
+  double stop_after_s;  /* > 0: checkpoint and stop after this many seconds of this call */
+} e13_checkpoint;
+
+/* e13_search that survives being stopped (replaces E13_CKPT / E13_CKPT_SEC /
+   <ckpt>.stop of src/e13gpu.py:349-409, 462-465).  Between epochs the whole
+   state of a search is on the device: the frontier stack, the job's counters
+   and its survivor records.  That state is written to the slot the pointer
+   file does not name, and only then is the pointer file replaced (write, fsync,
+   rename), so a crash during a save keeps the previous checkpoint.  A save
+   happens every interval_s, when the file <path>.stop appears (looked for once
+   a second; one left from an earlier clean stop is removed at the start), and
+   after stop_after_s.  The last two stop the search: E13_STOPPED, with the
+   counts so far in *counts and *nsurv.  If the pointer file exists at the
+   start, the search resumes from its slot.  A finished search removes the
+   checkpoint files and returns as e13_search does.  wall_s (may be NULL): wall
+   seconds of the search over all calls; frontier (may be NULL): frontier nodes
+   left at the stop (0 when finished). */
+int e13_search_resumable(e13_ctx *ctx, const e13_job *job, const e13_tuning *tuning, const e13_checkpoint *ck,
+                         e13_counts *counts, e13_survivor *surv, int surv_cap, int *nsurv, double *wall_s,
+                         int64_t *frontier);
 
 /* ---- serving: many searches in one persistent kernel ---- */
 

@@ -102,3 +102,18 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(E.E13Error) as ei:
         E.Context(0)
     assert ei.value.code in (-11, -5)
+
+
+def test_resumable_search_checks_its_arguments():
+    """e13_search_resumable rejects a missing context or checkpoint before
+    touching a device or a file."""
+    import ctypes
+    base = O.load_machine("erdos_14.txt")
+    r, job = E.setup(base, 13, free_cells=["D0", "G0", "K0", "K1", "L1", "M1"], lo=10, hi=13)
+    counts, ns = E.Counts(), ctypes.c_int()
+    ck = E.Checkpoint(b"/nonexistent/ckpt", b"cfg", 0.0, 0.0)
+    L = E.lib()
+    assert L.e13_search_resumable(None, ctypes.byref(job), None, ctypes.byref(ck), ctypes.byref(counts), None, 0,
+                                  ctypes.byref(ns), None, None) == -1
+    assert L.e13_search_resumable(None, ctypes.byref(job), None, None, ctypes.byref(counts), None, 0,
+                                  ctypes.byref(ns), None, None) == -1
