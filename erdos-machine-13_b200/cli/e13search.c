@@ -6,6 +6,7 @@
      e13search delete machine.txt FMAX X...
      e13search free machine.txt X CELL...
      e13search freesym machine.txt X LO HI CELL...
+     e13search estimate machine.txt PROBES X FMAX LO HI [CELL...]
 
    Survivors go to stdout in the reference's format, one summary line per X to
    stderr.  Environment: E13_DEVICE (CUDA device, default 0), E13_KERNEL
@@ -198,6 +199,36 @@ int main(int argc, char **argv) {
     rc = run_one(ctx, &job, &tu, (ckpath && ckpath[0]) ? &ck : NULL);
     e13_ctx_destroy(ctx);
     return rc == E13_STOPPED ? 3 : (rc ? 1 : 0);
+  }
+  if (!strcmp(mode, "estimate")) {
+    /* src/e13search.c:473-510: LO < 0 is no symmetry; cells make it a free search */
+    if (argc < 8) return 1;
+    long probes = atol(argv[3]);
+    int X = atoi(argv[4]), fmax = atoi(argv[5]), lo = atoi(argv[6]), hi = atoi(argv[7]);
+    uint8_t freebase[E13_MAXCELLS] = {0};
+    for (int i = 8; i < argc; i++) {
+      int c = 2 * (argv[i][0] - 'A') + (argv[i][1] - '0');
+      if (c >= 0 && c < E13_MAXCELLS) freebase[c] = 1;
+    }
+    e13_job job;
+    int rc = e13_setup(base, nq0, X, fmax, argc > 8 ? freebase : NULL, lo >= 0 ? lo : -1, hi, &job);
+    if (rc) return 1;
+    const char *seed_env = getenv("E13_SEED");
+    e13_ctx *ctx = open_ctx();
+    e13_estimate_out eo;
+    double w0 = now_s();
+    rc = e13_estimate(ctx, &job, probes, seed_env ? strtoull(seed_env, NULL, 10) : 0, &eo, NULL);
+    double wall = now_s() - w0;
+    e13_ctx_destroy(ctx);
+    if (rc) {
+      fprintf(stderr, "estimate failed (error %d)\n", rc);
+      return 1;
+    }
+    static const char *name[4] = {"leaves", "nodes", "steps", "survivors"};
+    printf("estimate X=%d budget=%d probes=%ld wall=%.1fs\n", X, job.budget, probes, wall);
+    for (int j = 0; j < 4; j++)
+      printf("  %-9s %.3e  (+- %.1e standard error)\n", name[j], eo.mean[j], eo.std_error[j]);
+    return 0;
   }
   fprintf(stderr, "unknown mode %s\n", mode);
   return 1;

@@ -44,6 +44,10 @@ class Checkpoint(ctypes.Structure):
                 ("stop_after_s", ctypes.c_double)]
 
 
+class EstimateOut(ctypes.Structure):
+    _fields_ = [("mean", ctypes.c_double * 4), ("std_error", ctypes.c_double * 4), ("probes", ctypes.c_int64)]
+
+
 class Job(ctypes.Structure):
     _fields_ = [("X", ctypes.c_int32), ("nq", ctypes.c_int32), ("tab", ctypes.c_int32 * E13_MAXCELLS),
                 ("budget", ctypes.c_int32), ("nforced", ctypes.c_int32), ("sym_lo", ctypes.c_int32),
@@ -138,6 +142,8 @@ def lib():
         L.e13_search_resumable.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Checkpoint), P(Counts),
                                            P(Survivor), I, P(I), P(ctypes.c_double), P(ctypes.c_int64)]
         L.e13_last_stats.argtypes = [ctypes.c_void_p, P(Stats)]
+        L.e13_estimate.argtypes = [ctypes.c_void_p, P(Job), ctypes.c_int64, ctypes.c_uint64, P(EstimateOut),
+                                   P(ctypes.c_double)]
         L.e13_autotune.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Tuning), P(ctypes.c_double)]
         L.e13_serve_create.argtypes = [ctypes.c_void_p, P(Tuning), ctypes.c_int64, P(ctypes.c_void_p)]
         L.e13_serve_destroy.argtypes = [ctypes.c_void_p]
@@ -164,7 +170,7 @@ def lib():
 
 EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine", "e13_setup",
             "e13_format_survivor", "e13_format_summary", "e13_default_tuning", "e13_ctx_create", "e13_ctx_destroy",
-            "e13_search", "e13_search_resumable", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
+            "e13_search", "e13_search_resumable", "e13_estimate", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
             "e13_format_recheck", "e13_format_deep", "e13_raw_run", "e13_autotune", "e13_check_noalloc",
             "e13_serve_create", "e13_serve_destroy", "e13_serve_clock", "e13_serve_submit", "e13_serve_step",
             "e13_serve_pending", "e13_serve_survivors", "e13_serve_stats"]
@@ -265,6 +271,17 @@ class Context:
         if r not in (0, -7, STOPPED):
             raise E13Error(r, "e13_search_resumable")
         return r, counts, [surv[i] for i in range(min(ns.value, surv_cap))], wall.value, left.value
+
+    def estimate(self, job: Job, probes: int, seed: int = 0, per_probe: bool = False):
+        """Knuth size estimate of the search for `job`; returns (EstimateOut,
+        per-probe [leaves, nodes, steps, survivors] rows or None)."""
+        out = EstimateOut()
+        buf = (ctypes.c_double * (4 * probes))() if per_probe else None
+        r = lib().e13_estimate(self.h, ctypes.byref(job), probes, seed, ctypes.byref(out), buf)
+        if r:
+            raise E13Error(r, "e13_estimate")
+        rows = [list(buf[4 * p: 4 * p + 4]) for p in range(probes)] if per_probe else None
+        return out, rows
 
     def autotune(self, job: Job, start: Tuning | None = None):
         """Coordinate-descent tuning of the persistent kernel on `job`; returns (Tuning, best ms)."""

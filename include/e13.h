@@ -194,6 +194,26 @@ int e13_search_resumable(e13_ctx *ctx, const e13_job *job, const e13_tuning *tun
                          e13_counts *counts, e13_survivor *surv, int surv_cap, int *nsurv, double *wall_s,
                          int64_t *frontier);
 
+/* ---- size estimate of a search ---- */
+
+typedef struct e13_estimate_out {
+  double mean[4];       /* leaves, nodes, steps, survivors: the average weighted count over the probes */
+  double std_error[4];  /* standard error of each mean (the reference's "+-") */
+  int64_t probes;
+} e13_estimate_out;
+
+/* Knuth's random-probe estimate of the search for `job` (src/e13search.c:256-313
+   probe, :473-510 estimate): each probe follows one random path from the
+   root, runs every child of every fork on it, and continues into a live
+   child drawn at random.  Probe p draws from the splitmix64 stream the
+   reference gives its OpenMP thread p (start mix(0x5EED0000 + p + (seed << 20)),
+   seed = E13_SEED), so every probe's counts depend only on (seed, p).
+   per_probe (may be NULL): 4 doubles per probe, leaves, nodes, steps,
+   survivors.  No counterpart of the per-probe layout in the reference, which
+   sums per thread. */
+int e13_estimate(e13_ctx *ctx, const e13_job *job, int64_t probes, uint64_t seed, e13_estimate_out *out,
+                 double *per_probe);
+
 /* ---- serving: many searches in one persistent kernel ---- */
 
 /* Continuous batching of search jobs (no counterpart in the reference, which

@@ -642,6 +642,92 @@ int oracle_deep_line(const char *line, int nmax, char *out, int olen) {
 
 /* Draw k (1-based) of splitmix64 from `seed`: the generator's state after k
    increments is seed + k * golden, so any draw can be made directly. */
+/* ------------------------------------------------------------------ */
+/* Knuth size estimate (e13search.c:256-313 probe, :473-510 estimate)   */
+
+/* Start of the splitmix64 stream the reference gives OpenMP thread k
+   (e13search.c:486-491): the state is the draw at 0x5EED0000 + k + (seed << 20). */
+uint64_t oracle_probe_stream(uint64_t seed, uint64_t k) {
+  uint64_t s = 0x5EED0000ULL + k + (seed << 20);
+  return mix_next(&s);
+}
+
+/* One probe: a random root-to-leaf path; every child of a fork on the path
+   runs to its next event and the path continues into a live child drawn
+   from *rng.  Adds the weighted counts to out[0..3] = leaves, nodes, steps,
+   survivors, in the reference's order of additions. */
+void oracle_probe(const int *tab0, int nq, int budget, int sym_lo, int sym_hi, int sym_n0, uint64_t *rng,
+                  double *out) {
+  oracle_keys(NULL, NULL);
+  OWalk w;
+  memset(&w, 0, sizeof w);
+  w.nq = nq;
+  w.sym_lo = sym_lo;
+  w.sym_hi = sym_hi;
+  int tab[2 * O_MAXQ];
+  unsigned char read[2 * O_MAXQ];
+  for (int i = 0; i < 2 * O_MAXQ; i++) tab[i] = i < 2 * nq ? tab0[i] : O_HALT;
+  memset(read, 0, sizeof read);
+  int nintro = sym_n0;
+  double wt = 1.0;
+  OSim *s = (OSim *)malloc(sizeof(OSim) * (4 * O_MAXQ + 2));
+  OSim *kids = s + 1;
+  osim_blank(s);
+  int i = osim_advance(s, tab, read);
+  out[1] += 1;
+  out[2] += (double)s->t;
+  if (i < 0) {
+    out[0] += 1;
+    if (i == O_SURVIVED) out[3] += 1;
+    free(s);
+    return;
+  }
+  for (;;) {
+    int orig = tab[i], vals[4 * O_MAXQ + 1], nbs[4 * O_MAXQ + 1], nis[4 * O_MAXQ + 1], k = 0;
+    if (orig != O_FREE) {
+      vals[k] = orig;
+      nbs[k] = budget;
+      nis[k] = nintro;
+      k++;
+    }
+    if (orig == O_FREE || budget > 0) {
+      for (int v = 0; v < 4 * nq; v++) {
+        int ni = sym_after(&w, v, nintro);
+        if (v == orig || ni < 0) continue;
+        vals[k] = v;
+        nbs[k] = orig == O_FREE ? budget : budget - 1;
+        nis[k] = ni;
+        k++;
+      }
+    }
+    int live[4 * O_MAXQ + 1], nlive = 0;
+    read[i] = 1;
+    for (int c = 0; c < k; c++) {
+      kids[c] = *s;
+      tab[i] = vals[c];
+      long t0 = kids[c].t;
+      int r = osim_advance(&kids[c], tab, read);
+      out[1] += wt;
+      out[2] += wt * (double)(kids[c].t - t0);
+      if (r < 0) {
+        out[0] += wt;
+        if (r == O_SURVIVED) out[3] += wt;
+      } else {
+        live[nlive++] = c;
+      }
+    }
+    if (!nlive) break;
+    int c = live[mix_next(rng) % (uint64_t)nlive];
+    wt *= nlive;
+    tab[i] = vals[c];
+    budget = nbs[c];
+    nintro = nis[c];
+    *s = kids[c];
+    i = osim_advance(s, tab, read); /* the same unread cell, no steps */
+  }
+  free(s);
+}
+
 static uint64_t mix_draw(uint64_t seed, uint64_t k) {
   uint64_t s = seed + (k - 1) * 0x9E3779B97F4A7C15ULL;
   return mix_next(&s);

@@ -16,6 +16,13 @@ Outputs (all small text / gzip files, committed):
   deep/*.txt(.gz)          deep.c outputs (V1 at 15, V2, erdos_14)
   mutants.txt              e13search mutant on erdos_14
   base_erdos14.txt         e13search base on erdos_14
+  estimate_ref.json        e13search estimate printed by the reference binary
+                           on one OpenMP thread (so every probe draws from
+                           thread 0's stream, in order): args, E13_SEED and
+                           the four result lines
+
+``python tests/golden/make_golden.py [REFERENCE_DIR] estimates`` remakes only
+estimate_ref.json.
 
 Every number comes from the reference's own result logs except the step
 counts marked "steps_source": "reference binary" -- those were printed by the
@@ -34,7 +41,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ARGS = [a for a in sys.argv[1:] if a != "estimates"]
+REF = ARGS[0] if ARGS else "/root/reference"
 RES = os.path.join(REF, "results")
 REFBIN = os.path.join(REPO, "oracle", "_ref", "e13search")
 
@@ -97,6 +105,28 @@ def summaries_from_text(text):
         if m:
             out.append(dict(X=int(m.group(1)), steps=int(m.group(4)) if m.group(4) else None))
     return out
+
+
+ESTIMATE_CASES = [
+    (["estimate", ERDOS14, "2000", "8", "2", "-1", "-1"], 0),
+    (["estimate", ERDOS14, "1000", "11", "3", "-1", "-1"], 0),
+    (["estimate", ERDOS14, "3000", "13", "0", "10", "13", "D0", "G0", "K0", "K1", "L1", "M1"], 7),
+    (["estimate", ERDOS14, "2000", "13", "0", "-1", "-1", "D0", "G0", "K0", "K1", "L1", "M1"], 3),
+]
+
+
+def estimates():
+    """The reference's estimate mode (src/e13search.c:473-510) on one thread."""
+    out = []
+    for args, seed in ESTIMATE_CASES:
+        run = [REFBIN, args[0], os.path.join(HERE, "machines", args[1])] + args[2:]
+        r = subprocess.run(run, capture_output=True, text=True, check=True,
+                           env=dict(os.environ, OMP_NUM_THREADS="1", E13_SEED=str(seed)))
+        lines = r.stdout.splitlines()
+        head = re.sub(r" wall=\S+", "", lines[0])
+        out.append(dict(args=args, seed=seed, threads=1, header=head, lines=lines[1:5]))
+    with open(os.path.join(HERE, "estimate_ref.json"), "w") as f:
+        json.dump(out, f, indent=1)
 
 
 def main():
@@ -227,4 +257,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if "estimates" in sys.argv[1:]:
+        estimates()
+    else:
+        main()
+        estimates()

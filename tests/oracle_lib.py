@@ -44,6 +44,10 @@ def lib():
         L.oracle_deep_line.argtypes = [ctypes.c_char_p, I, ctypes.c_char_p, I]
         L.oracle_raw_tables.argtypes = [ctypes.c_uint64, ctypes.c_long, I, ctypes.c_char_p]
         L.oracle_raw_run.argtypes = [ctypes.c_char_p, ctypes.c_long, I, ctypes.c_long, P(ctypes.c_longlong)]
+        L.oracle_probe_stream.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+        L.oracle_probe_stream.restype = ctypes.c_uint64
+        L.oracle_probe.argtypes = [P(I), I, I, I, I, I, P(ctypes.c_uint64), P(ctypes.c_double)]
+        L.oracle_probe.restype = None
         _lib = L
     return _lib
 
@@ -189,3 +193,53 @@ def raw_run(codes: bytes, n: int, nq: int = 13, max_steps: int = 1 << 18):
     out = (ctypes.c_longlong * (4 * n))()
     lib().oracle_raw_run(codes, n, nq, max_steps, out)
     return [list(out[4 * i: 4 * i + 4]) for i in range(n)]
+
+
+def probe(job: Job, rng_state: int):
+    """One estimator probe (src/e13search.c:262-313) from the given splitmix64
+    state; returns ([leaves, nodes, steps, survivors], the state after it)."""
+    tab = (ctypes.c_int * 32)(*(job.tab + [HALT] * (32 - len(job.tab))))
+    out = (ctypes.c_double * 4)()
+    st = ctypes.c_uint64(rng_state)
+    lib().oracle_probe(tab, job.nq, max(job.budget, 0), job.sym_lo, job.sym_hi, job.sym_n0, ctypes.byref(st), out)
+    return list(out), st.value
+
+
+def probe_stream(seed: int, k: int) -> int:
+    """The splitmix64 state the reference gives OpenMP thread k (src/e13search.c:486-491)."""
+    return lib().oracle_probe_stream(seed, k)
+
+
+def estimate_per_probe(job: Job, probes: int, seed: int = 0):
+    """Per-probe results with probe p on stream k = p (the device's layout)."""
+    return [probe(job, probe_stream(seed, p))[0] for p in range(probes)]
+
+
+def estimate_lines(job: Job, probes: int, seed: int = 0) -> list[str]:
+    """The four result lines the reference prints for `estimate` run on one
+    OpenMP thread (src/e13search.c:505-509): all probes on thread 0's stream."""
+    st = probe_stream(seed, 0)
+    rows = []
+    for _ in range(probes):
+        o, st = probe(job, st)
+        rows.append(o)
+    return lines_from_rows(rows)
+
+
+def lines_from_rows(rows) -> list[str]:
+    """Mean and standard error lines of per-probe results, summed in order
+    (src/e13search.c:500-509)."""
+    import math
+    n = len(rows)
+    s, q = [0.0] * 4, [0.0] * 4
+    for o in rows:
+        for j in range(4):
+            s[j] += o[j]
+            q[j] += o[j] * o[j]
+    lines = []
+    for j, name in enumerate(("leaves", "nodes", "steps", "survivors")):
+        m = s[j] / n
+        var = q[j] / n - m * m
+        se = math.sqrt(var / n) if var > 0 else 0.0
+        lines.append("  %-9s %.3e  (+- %.1e standard error)" % (name, m, se))
+    return lines

@@ -186,3 +186,36 @@ def test_raw_run_small_known_cases():
     # A0 = 0LA: walks left over blanks, leaves at -64 after 63 counted steps
     codes = bytes([0, 0]) + bytes([0] * 24)
     assert O.raw_run(codes, 1, nq=13)[0] == [63, 1, -64, 0]
+
+
+def _estimate_job(case):
+    args = case["args"]
+    X, fmax, lo, hi = int(args[3]), int(args[4]), int(args[5]), int(args[6])
+    cells = args[7:] or None
+    base = O.load_machine(args[1])
+    r, job = O.setup(base, X, fmax=fmax, free_cells=cells, lo=lo if lo >= 0 else -1, hi=hi)
+    assert r >= 0
+    return job, int(args[2])
+
+
+def test_estimate_equals_reference_binary():
+    """The restated probe() draws and adds exactly as the reference: on one
+    thread's stream its printed estimate is the reference binary's, digit for
+    digit (fixtures made by tests/golden/make_golden.py)."""
+    import json
+    cases = json.load(open(os.path.join(GOLD, "estimate_ref.json")))
+    assert len(cases) >= 4
+    for case in cases:
+        job, probes = _estimate_job(case)
+        assert case["header"].startswith(f"estimate X={job.X} budget={job.budget} probes={probes}")
+        assert O.estimate_lines(job, probes, case["seed"]) == case["lines"], case["args"]
+
+
+def test_estimate_probe_streams_are_independent():
+    """Per-probe streams: probe p's result depends only on (seed, p)."""
+    base = O.load_machine("erdos_14.txt")
+    r, job = O.setup(base, 11, fmax=3)
+    a = O.estimate_per_probe(job, 50, seed=5)
+    b = [O.probe(job, O.probe_stream(5, p))[0] for p in reversed(range(50))][::-1]
+    assert a == b
+    assert O.estimate_per_probe(job, 50, seed=6) != a
