@@ -774,3 +774,336 @@ void oracle_raw_run(const unsigned char *codes, long n, int nq, long max_steps, 
     out[4 * m + 3] = ones;
   }
 }
+
+/* ------------------------------------------------------------------ */
+/* check.py: hash-free stages 1..11 and crafted stage starts            */
+/* (src/check.py:1-173), with check.py's unbounded tape and its text     */
+
+#define CK_NMAX 11 /* check.py:20 */
+#define CK_MMAX 40 /* check.py:21 */
+
+enum { CK_STOP = 0, CK_HALT = 1, CK_LIMIT = 2 };
+static const char *const CK_RES[3] = {"stop", "halt", "limit"};
+
+/* a tape that grows to whatever cells the machine visits */
+typedef struct {
+  unsigned char *b;
+  long lo, n; /* cells lo .. lo + n - 1 */
+} CkTape;
+
+static int ck_get(const CkTape *t, long c) { return c >= t->lo && c < t->lo + t->n ? t->b[c - t->lo] : 0; }
+
+static void ck_set(CkTape *t, long c, int v) {
+  if (c < t->lo || c >= t->lo + t->n) {
+    if (!v) return;
+    long lo = t->lo, hi = t->lo + t->n;
+    long want_lo = c < lo ? c - (t->n + 64) : lo, want_hi = c >= hi ? c + (t->n + 64) : hi;
+    unsigned char *nb = (unsigned char *)calloc((size_t)(want_hi - want_lo), 1);
+    if (t->n) memcpy(nb + (lo - want_lo), t->b, (size_t)t->n);
+    free(t->b);
+    t->b = nb;
+    t->lo = want_lo;
+    t->n = want_hi - want_lo;
+  }
+  t->b[c - t->lo] = (unsigned char)v;
+}
+
+/* the ones at cells < -2, ascending (check.py:51-52) */
+static int ck_counter(const CkTape *t, long *cells, int cap) {
+  int k = 0;
+  for (long c = t->lo; c < -2 && c < t->lo + t->n; c++)
+    if (t->b[c - t->lo]) {
+      if (k < cap) cells[k] = c;
+      k++;
+    }
+  return k;
+}
+
+typedef struct {
+  int stage_one; /* stage 1: the block alone (check.py:85-86) */
+  int crafted;   /* crafted start: head must be exactly hh (check.py:142-146) */
+  long size, h0, hh;
+  int s0;
+} CkStop;
+
+static int ck_is_block(const CkTape *t, long size, long ones_ge) {
+  if (ones_ge != size) return 0;
+  for (long c = -1; c < size - 1; c++)
+    if (!ck_get(t, c)) return 0;
+  return 1;
+}
+
+static int ck_stop(const CkTape *t, long ones_ge, long head, int st, const CkStop *s) {
+  if (ones_ge != s->size) return 0;
+  if (!s->stage_one) {
+    if (st != s->s0) return 0;
+    if (s->crafted ? head != s->hh : (head != s->h0 && head - s->size != s->h0 - 2)) return 0;
+  }
+  return ck_is_block(t, s->size, ones_ge);
+}
+
+/* run_tracked (check.py:55-77): rows[i] = write | right << 1 | next << 2, or -1 halt */
+static int ck_run(const int *rows, CkTape *t, long *head, int *st, const CkStop *s, long limit, long *steps) {
+  long ones_ge = 0;
+  for (long c = -2; c < t->lo + t->n; c++) ones_ge += ck_get(t, c);
+  for (long k = 0; k < limit; k++) {
+    if (ck_stop(t, ones_ge, *head, *st, s)) {
+      *steps = k;
+      return CK_STOP;
+    }
+    int sym = ck_get(t, *head);
+    int r = rows[2 * *st + sym];
+    if (r < 0) {
+      *steps = k;
+      return CK_HALT;
+    }
+    int w = r & 1;
+    if (w && !sym) {
+      ck_set(t, *head, 1);
+      if (*head >= -2) ones_ge++;
+    } else if (sym && !w) {
+      ck_set(t, *head, 0);
+      if (*head >= -2) ones_ge--;
+    }
+    *head += (r & 2) ? 1 : -1;
+    *st = r >> 2;
+  }
+  *steps = limit;
+  return CK_LIMIT;
+}
+
+static int ck_no_two(long m) {
+  while (m) {
+    if (m % 3 == 2) return 0;
+    m /= 3;
+  }
+  return 1;
+}
+
+typedef struct {
+  char *s;
+  size_t len, cap;
+} CkBuf;
+
+static void ck_put(CkBuf *b, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+#include <stdarg.h>
+static void ck_put(CkBuf *b, const char *fmt, ...) {
+  for (;;) {
+    va_list ap;
+    va_start(ap, fmt);
+    int n = vsnprintf(b->s + b->len, b->cap - b->len, fmt, ap);
+    va_end(ap);
+    if (n >= 0 && (size_t)n < b->cap - b->len) {
+      b->len += (size_t)n;
+      return;
+    }
+    b->cap = 2 * b->cap + (size_t)(n > 0 ? n : 256) + 256;
+    b->s = (char *)realloc(b->s, b->cap);
+  }
+}
+
+/* Python's repr of a tuple of ints */
+static void ck_tuple(CkBuf *b, const long *v, int n) {
+  ck_put(b, "(");
+  for (int i = 0; i < n; i++) ck_put(b, i ? ", %ld" : "%ld", v[i]);
+  ck_put(b, n == 1 ? ",)" : ")");
+}
+
+#define CK_CAP 4096 /* counter cells kept per stage start */
+
+typedef struct {
+  int st;
+  long head, total;
+  int ncnt;
+  long *cnt;
+} CkStart;
+
+static int ck_same(const long *a, int na, const long *b, int nb) {
+  return na == nb && (na == 0 || !memcmp(a, b, sizeof(long) * (size_t)na));
+}
+
+/* One placement: check.py's check() body (:102-162) for a table with its
+   halt placed; appends "   halt@<place>: ..." to b. */
+static void ck_placement(const int *rows, int place, CkBuf *b) {
+  CkTape tp = {0, 0, 0};
+  CkStart starts[CK_NMAX + 1];
+  int nstarts = 0;
+  long head = 0, total = 0;
+  int st = 0;
+  char place_s[16];
+  if (place < 0) snprintf(place_s, sizeof place_s, "None");
+  else snprintf(place_s, sizeof place_s, "%d", place);
+  for (int n = 1; n <= CK_NMAX; n++) {
+    CkStop s = {nstarts == 0, 0, 1L << n, nstarts ? starts[0].head : 0, 0, nstarts ? starts[0].st : 0};
+    long t = 0;
+    int res = ck_run(rows, &tp, &head, &st, &s, 40L * (1L << (2 * n)) + 1000, &t);
+    total += t;
+    if (res != CK_STOP) {
+      ck_put(b, "   halt@%s: FAIL stage %d: %s at step %ld\n", place_s, n, CK_RES[res], total);
+      goto out;
+    }
+    starts[nstarts].st = st;
+    starts[nstarts].head = head;
+    starts[nstarts].total = total;
+    starts[nstarts].cnt = (long *)malloc(sizeof(long) * CK_CAP);
+    starts[nstarts].ncnt = ck_counter(&tp, starts[nstarts].cnt, CK_CAP);
+    nstarts++;
+  }
+  {
+    /* counter consistency (:116-126): cnt[c] = the counter at the first start with c */
+    int have[3] = {0, 0, 0}, first[3] = {0, 0, 0};
+    char bad[96] = "";
+    for (int i = 0; i < nstarts; i++) {
+      int n = i + 1, c = 0;
+      for (int k = 1; k < n; k++) c += ck_no_two(1L << k);
+      if (have[c] && !ck_same(starts[first[c]].cnt, starts[first[c]].ncnt, starts[i].cnt, starts[i].ncnt))
+        snprintf(bad, sizeof bad, "counter differs within c=%d at n=%d", c, n);
+      if (!have[c]) {
+        have[c] = 1;
+        first[c] = i;
+      }
+    }
+    int ndistinct = 0, nkeys = 0;
+    for (int c = 0; c < 3; c++) {
+      if (!have[c]) continue;
+      nkeys++;
+      int dup = 0;
+      for (int d = 0; d < c; d++)
+        if (have[d] && ck_same(starts[first[d]].cnt, starts[first[d]].ncnt, starts[first[c]].cnt, starts[first[c]].ncnt))
+          dup = 1;
+      ndistinct += !dup;
+    }
+    if (ndistinct != nkeys) snprintf(bad, sizeof bad, "counter equal for different c");
+    if (bad[0]) {
+      ck_put(b, "   halt@%s: FAIL %s\n", place_s, bad);
+      goto out;
+    }
+    const int s0 = starts[0].st;
+    const long h0 = starts[0].head;
+    int absolute = 1;
+    for (int i = 0; i < nstarts; i++)
+      if (starts[i].head != h0) absolute = 0;
+    /* crafted stage starts (:128-156) */
+    CkBuf fails = {0, 0, 0};
+    int nfails = 0;
+    long *got = (long *)malloc(sizeof(long) * CK_CAP);
+    for (int c = 0; c < 3; c++) {
+      if (!have[c]) continue;
+      for (long m = 2; m <= CK_MMAX; m++) {
+        CkTape ct = {0, 0, 0};
+        const CkStart *cs = &starts[first[c]];
+        for (int i = 0; i < cs->ncnt; i++) ck_set(&ct, cs->cnt[i], 1);
+        for (long k = -1; k < m - 1; k++) ck_set(&ct, k, 1);
+        long hd = absolute ? h0 : h0 - 2 + m;
+        int cst = s0;
+        const long nxt = 2 * m;
+        const int want_c = ck_no_two(m) ? c + 1 : c;
+        const int want_halt = ck_no_two(m) && c == 2;
+        CkStop s = {0, 1, nxt, h0, absolute ? h0 : h0 - 2 + nxt, s0};
+        long t = 0;
+        int res = ck_run(rows, &ct, &hd, &cst, &s, 40 * m * m + 5000, &t);
+        char msg[1024] = "";
+        if (want_halt) {
+          if (res != CK_HALT) snprintf(msg, sizeof msg, "expected halt, got %s", CK_RES[res]);
+        } else if (res != CK_STOP) {
+          snprintf(msg, sizeof msg, "expected stage 2m, got %s at %ld", CK_RES[res], t);
+        } else {
+          int ng = ck_counter(&ct, got, CK_CAP);
+          if (want_c < 3 && have[want_c]) {
+            const CkStart *ts = &starts[first[want_c]];
+            if (!ck_same(got, ng, ts->cnt, ts->ncnt)) {
+              CkBuf mb = {0, 0, 0};
+              ck_put(&mb, "counter ");
+              ck_tuple(&mb, got, ng);
+              ck_put(&mb, " != c=%d ", want_c);
+              ck_tuple(&mb, ts->cnt, ts->ncnt);
+              snprintf(msg, sizeof msg, "%s", mb.s);
+              free(mb.s);
+            }
+          } else {
+            for (int d = 0; d < 3; d++)
+              if (have[d] && ck_same(got, ng, starts[first[d]].cnt, starts[first[d]].ncnt))
+                snprintf(msg, sizeof msg, "counter for c=3 equals an earlier one");
+          }
+        }
+        free(ct.b);
+        if (msg[0]) {
+          if (nfails < 4) ck_put(&fails, nfails ? ", (%d, %ld, '%s')" : "(%d, %ld, '%s')", c, m, msg);
+          nfails++;
+        }
+      }
+    }
+    free(got);
+    ck_put(b, "   halt@%s: %s stages ok to n=%d (step %ld); counters {", place_s, nfails ? "FAIL" : "PASS", CK_NMAX,
+           starts[nstarts - 1].total);
+    int firstkey = 1;
+    for (int c = 0; c < 3; c++) {
+      if (!have[c]) continue;
+      ck_put(b, firstkey ? "%d: " : ", %d: ", c);
+      ck_tuple(b, starts[first[c]].cnt, starts[first[c]].ncnt);
+      firstkey = 0;
+    }
+    ck_put(b, "}; crafted fails %d: [%s]\n", nfails, fails.s ? fails.s : "");
+    free(fails.s);
+  }
+out:
+  for (int i = 0; i < nstarts; i++) free(starts[i].cnt);
+  free(tp.b);
+}
+
+/* check.py's output for one input line (its __main__, :165-173): the line
+   (stripped), then a verdict line per placement of the halt.  Returns the
+   text length (truncated to outlen - 1), 0 if the line has no table. */
+int oracle_check_line(const char *line, char *out, int outlen) {
+  const char *tb = strstr(line, "table=");
+  if (!tb || outlen < 1) return 0;
+  int rows[2 * O_MAXQ], unread[2 * O_MAXQ], nun = 0, ncell = 0, nhalt = 0;
+  const char *q = tb + 6;
+  while (*q == ' ' || *q == '\t') q++;
+  while (*q && *q != '\n' && *q != '\r' && ncell < 2 * O_MAXQ) {
+    while (*q == ' ' || *q == '\t') q++;
+    if (*q == '|') {
+      q++;
+      continue;
+    }
+    if (!*q || *q == '\n' || *q == '\r') break;
+    int un = 0;
+    if (*q == '?') {
+      un = 1;
+      q++;
+    }
+    if (*q == '-') {
+      rows[ncell] = -1;
+      nhalt++;
+      q += 3;
+    } else {
+      int w = *q++ - '0';
+      int right = *q++ == 'R';
+      int nx = (int)strtol(q, (char **)&q, 10);
+      rows[ncell] = w | (right << 1) | (nx << 2);
+    }
+    if (un) unread[nun++] = ncell;
+    ncell++;
+  }
+  CkBuf b = {0, 0, 0};
+  /* the line, stripped */
+  const char *s = line, *e = line + strlen(line);
+  while (*s == ' ' || *s == '\t' || *s == '\n' || *s == '\r') s++;
+  while (e > s && (e[-1] == ' ' || e[-1] == '\t' || e[-1] == '\n' || e[-1] == '\r')) e--;
+  ck_put(&b, "%.*s\n", (int)(e - s), s);
+  if (nhalt) {
+    ck_placement(rows, -1, &b);
+  } else {
+    for (int i = 0; i < nun; i++) {
+      int r2[2 * O_MAXQ];
+      memcpy(r2, rows, sizeof r2);
+      r2[unread[i]] = -1;
+      ck_placement(r2, unread[i], &b);
+    }
+  }
+  int n = (int)b.len < outlen - 1 ? (int)b.len : outlen - 1;
+  memcpy(out, b.s, (size_t)n);
+  out[n] = 0;
+  free(b.s);
+  return n;
+}

@@ -16,13 +16,16 @@ Outputs (all small text / gzip files, committed):
   deep/*.txt(.gz)          deep.c outputs (V1 at 15, V2, erdos_14)
   mutants.txt              e13search mutant on erdos_14
   base_erdos14.txt         e13search base on erdos_14
+  check/*.txt              src/check.py's shipped outputs (the survivor line,
+                           then one "halt@<place>: PASS|FAIL ..." line per
+                           placement), copied from the reference's results
   estimate_ref.json        e13search estimate printed by the reference binary
                            on one OpenMP thread (so every probe draws from
                            thread 0's stream, in order): args, E13_SEED and
                            the four result lines
 
 ``python tests/golden/make_golden.py [REFERENCE_DIR] estimates`` remakes only
-estimate_ref.json.
+estimate_ref.json, ``... checks`` only check/.
 
 Every number comes from the reference's own result logs except the step
 counts marked "steps_source": "reference binary" -- those were printed by the
@@ -41,7 +44,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-ARGS = [a for a in sys.argv[1:] if a != "estimates"]
+ARGS = [a for a in sys.argv[1:] if a not in ("estimates", "checks")]
 REF = ARGS[0] if ARGS else "/root/reference"
 RES = os.path.join(REF, "results")
 REFBIN = os.path.join(REPO, "oracle", "_ref", "e13search")
@@ -113,6 +116,26 @@ ESTIMATE_CASES = [
     (["estimate", ERDOS14, "3000", "13", "0", "10", "13", "D0", "G0", "K0", "K1", "L1", "M1"], 7),
     (["estimate", ERDOS14, "2000", "13", "0", "-1", "-1", "D0", "G0", "K0", "K1", "L1", "M1"], 3),
 ]
+
+
+CHECK_FILES = {
+    "erdos14.txt": "validation/check_erdos14.txt",
+    "f4_unread.txt": "1_local_edits/check_f4_unread.txt",
+    "counter_plus_f2.txt": "5_counter_plus/f2_f3/check_f2.txt",
+    "counter_plus_f3.txt": "5_counter_plus/f2_f3/check_f3.txt",
+    "counter_plus_cx.txt": "5_counter_plus/extra_cell/check_cx.txt",
+    "division_v2.txt": "4_division_6/v2/check_v2.txt",
+}
+
+
+def check_outputs():
+    """check.py's outputs as the reference ships them (comment lines dropped)."""
+    os.makedirs(os.path.join(HERE, "check"), exist_ok=True)
+    for name, src in CHECK_FILES.items():
+        with open(os.path.join(RES, src)) as f, open(os.path.join(HERE, "check", name), "w") as g:
+            for line in f:
+                if not line.startswith("#"):
+                    g.write(line)
 
 
 def estimates():
@@ -253,12 +276,15 @@ def main():
     shutil.copy(os.path.join(RES, "validation", "deep_base14.txt"), os.path.join(HERE, "deep", "deep_base14.txt"))
     shutil.copy(os.path.join(RES, "validation", "mutants.txt"), os.path.join(HERE, "mutants.txt"))
     shutil.copy(os.path.join(RES, "validation", "base_erdos14.txt"), os.path.join(HERE, "base_erdos14.txt"))
+    check_outputs()
     print(f"{len(searches)} searches, {len(verdicts)} recheck verdicts")
 
 
 if __name__ == "__main__":
     if "estimates" in sys.argv[1:]:
         estimates()
+    elif "checks" in sys.argv[1:]:
+        check_outputs()
     else:
         main()
         estimates()

@@ -48,6 +48,7 @@ def lib():
         L.oracle_probe_stream.restype = ctypes.c_uint64
         L.oracle_probe.argtypes = [P(I), I, I, I, I, I, P(ctypes.c_uint64), P(ctypes.c_double)]
         L.oracle_probe.restype = None
+        L.oracle_check_line.argtypes = [ctypes.c_char_p, ctypes.c_char_p, I]
         _lib = L
     return _lib
 
@@ -243,3 +244,22 @@ def lines_from_rows(rows) -> list[str]:
         se = math.sqrt(var / n) if var > 0 else 0.0
         lines.append("  %-9s %.3e  (+- %.1e standard error)" % (name, m, se))
     return lines
+
+
+def check_line(line: str) -> list[str]:
+    """check.py's output lines for one input line (src/check.py:165-173)."""
+    buf = ctypes.create_string_buffer(1 << 16)
+    n = lib().oracle_check_line(line.encode(), buf, len(buf))
+    return buf.value.decode().splitlines() if n else []
+
+
+def check_golden(path: str) -> list[tuple[str, list[str]]]:
+    """(input line, verdict lines) pairs of a shipped check.py output."""
+    pairs = []
+    for line in open(path):
+        line = line.rstrip("\n")
+        if "table=" in line:
+            pairs.append([line, []])
+        elif line.startswith("   halt@") and pairs:
+            pairs[-1][1].append(line)
+    return [(l, v) for l, v in pairs if v]

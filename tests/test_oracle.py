@@ -219,3 +219,20 @@ def test_estimate_probe_streams_are_independent():
     b = [O.probe(job, O.probe_stream(5, p))[0] for p in reversed(range(50))][::-1]
     assert a == b
     assert O.estimate_per_probe(job, 50, seed=6) != a
+
+
+def test_check_py_restatement_equals_shipped_outputs():
+    """The oracle's restatement of src/check.py prints, for every survivor
+    line of the reference's shipped check.py outputs, the same verdict lines
+    (stages to n = 11, counters per c, crafted-start fails)."""
+    import glob
+    files = sorted(glob.glob(os.path.join(GOLD, "check", "*.txt")))
+    assert len(files) == 6
+    n = 0
+    for f in files:
+        for line, verdicts in O.check_golden(f):
+            got = O.check_line(line)
+            assert got[0] == line.strip()
+            assert got[1:] == verdicts, (f, line[:80])
+            n += 1
+    assert n == 164
