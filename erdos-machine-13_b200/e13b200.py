@@ -142,6 +142,8 @@ def lib():
         L.e13_search_resumable.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Checkpoint), P(Counts),
                                            P(Survivor), I, P(I), P(ctypes.c_double), P(ctypes.c_int64)]
         L.e13_last_stats.argtypes = [ctypes.c_void_p, P(Stats)]
+        L.e13_check_crafted.argtypes = [ctypes.c_void_p, P(ctypes.c_char_p), I, ctypes.c_char_p, ctypes.c_size_t,
+                                        P(ctypes.c_size_t)]
         L.e13_estimate.argtypes = [ctypes.c_void_p, P(Job), ctypes.c_int64, ctypes.c_uint64, P(EstimateOut),
                                    P(ctypes.c_double)]
         L.e13_autotune.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Tuning), P(ctypes.c_double)]
@@ -171,7 +173,7 @@ def lib():
 EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine", "e13_setup",
             "e13_format_survivor", "e13_format_summary", "e13_default_tuning", "e13_ctx_create", "e13_ctx_destroy",
             "e13_search", "e13_search_resumable", "e13_estimate", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
-            "e13_format_recheck", "e13_format_deep", "e13_raw_run", "e13_autotune", "e13_check_noalloc",
+            "e13_format_recheck", "e13_format_deep", "e13_check_crafted", "e13_raw_run", "e13_autotune", "e13_check_noalloc",
             "e13_serve_create", "e13_serve_destroy", "e13_serve_clock", "e13_serve_submit", "e13_serve_step",
             "e13_serve_pending", "e13_serve_survivors", "e13_serve_stats"]
 
@@ -282,6 +284,22 @@ class Context:
             raise E13Error(r, "e13_estimate")
         rows = [list(buf[4 * p: 4 * p + 4]) for p in range(probes)] if per_probe else None
         return out, rows
+
+    def check_crafted(self, lines):
+        """src/check.py on the device: its output lines for these input lines."""
+        arr = (ctypes.c_char_p * max(len(lines), 1))(*[l.encode() for l in lines])
+        need = ctypes.c_size_t()
+        size = 1 << 16
+        for _ in range(2):
+            buf = ctypes.create_string_buffer(size)
+            r = lib().e13_check_crafted(self.h, arr, len(lines), buf, size, ctypes.byref(need))
+            if r == -1 and need.value > size:
+                size = need.value
+                continue
+            if r:
+                raise E13Error(r, "e13_check_crafted")
+            return buf.value.decode().splitlines()
+        raise E13Error(-1, "e13_check_crafted")
 
     def autotune(self, job: Job, start: Tuning | None = None):
         """Coordinate-descent tuning of the persistent kernel on `job`; returns (Tuning, best ms)."""

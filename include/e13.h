@@ -351,6 +351,23 @@ int e13_check_noalloc(int device, const e13_check_in *in, int n, int nmax, int m
    Returns 1 on success, 0 if the line has no table. */
 int e13_parse_survivor_line(const char *line, e13_check_in *in);
 
+/* ---- check.py: stages to 11 and crafted stage starts ---- */
+
+#define E13_CRAFTED_MAX_CELLS 256  /* counter cells recorded per stage start */
+
+/* src/check.py on the device, with its text.  lines: survivor lines as
+   check.py reads them (lines without "table=" are skipped).  For each, the
+   output holds the line (stripped) and one "   halt@<place>: PASS|FAIL ..."
+   line per placement of the halt: the table's own halt, else each never-read
+   ('?') cell in turn (src/check.py:102-162, :165-173).  out: a buffer of
+   out_len bytes, NUL-terminated; *needed (may be NULL) = the bytes the text
+   needs.  Returns E13_OK; E13_ERR_ARG if out is too small; E13_ERR_OVERFLOW
+   if a counter held more than E13_CRAFTED_MAX_CELLS ones (its text is then
+   not exact).  check.py's tape is unbounded; here a stage walk has cells
+   -2^22 .. 2^22 and a crafted run -2^18 .. 2^18, and a run that leaves them
+   is reported as "off tape" in place of check.py's outcome. */
+int e13_check_crafted(e13_ctx *ctx, const char *const *lines, int n, char *out, size_t out_len, size_t *needed);
+
 /* recheck.c's verdict text for one machine (src/recheck.c:71-99) from the
    device result; returns 1 if CONSISTENT. */
 int e13_format_recheck(const e13_check_out *o, int nmax, char *buf, size_t len);
