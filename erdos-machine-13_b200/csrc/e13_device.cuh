@@ -240,6 +240,7 @@ __device__ __forceinline__ int lane_act(Lane &L, u32 *__restrict__ tcol, const u
   const int widx = (p >> 5) * stride;
   const u32 word = tcol[widx];
   const u32 row = rcol[L.st * stride];
+  const u64 kk = keyb[p];  // loaded with the word and the row, used only on a flip
   const u32 sym = (word >> (p & 31)) & 1u;
   const u32 e = (row >> (sym << 4)) & 0x1FFu;
   if (e & kEntSpecial) {
@@ -262,9 +263,10 @@ __device__ __forceinline__ int lane_act(Lane &L, u32 *__restrict__ tcol, const u
   k = k < lim_t ? k : lim_t;
   k = k < room ? k : room;
   k = ((e & kEntSelf) && L.hb != L.tgt && k > 1) ? k : 1;
-  if ((e ^ sym) & 1u) {  // never on a self-loop cell
-    tcol[widx] = word ^ (1u << b);
-    L.hb ^= keyb[p];  // zero for cells < -2: those go to the counter hash
+  {  // the write, without a branch (a self-loop cell never flips)
+    const u32 flip = (e ^ sym) & 1u;
+    tcol[widx] = word ^ (flip << b);
+    L.hb ^= kk & (0ull - (u64)flip);  // keyb is zero for cells < -2: those go to the counter hash
   }
   const int np = p + (right ? k : -k);
   if ((unsigned)(np - 1) >= (unsigned)(kTapeCells - 2)) return kEvDead;  // head <= -64 or >= 1299

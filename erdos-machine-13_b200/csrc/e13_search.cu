@@ -464,8 +464,6 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
       if (rm) {
 #pragma unroll 1
         for (int it = 0; it < P.slice; ++it) {
-          // end the slice early once a quarter of the lanes wait for work
-          if ((it & 7) == 7 && __popc(__ballot_sync(kFull, status == kStRun)) < 24) break;
           if (status == kStRun) {
             int cell = 0;
             u32 e = 0;
@@ -502,9 +500,9 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
               status = kStIdle;
             }
           }
-          // every lane comes here each iteration (the loop bounds and the early
-          // exit are warp-uniform): rejoin the lanes that took rare branches so
-          // the next action issues once for the whole warp
+          // every lane comes here each iteration (the loop bounds are
+          // warp-uniform): rejoin the lanes that took rare branches so the next
+          // action issues once for the whole warp
           __syncwarp();
         }
         if (!PERSIST && status == kStRun && L.t - L.tseg >= P.step_cap) {
