@@ -228,8 +228,8 @@ def reference_arm(args, w, ws, rank, pg):
 
 
 def serving_bench(args, w, ws, rank, local, pg):
-    """configs[4] part 1: jobs arrive as a Poisson stream and join the running
-    persistent kernel as slots and frontier memory free up."""
+    """The serving workload: search jobs arrive as a Poisson stream and join the
+    running persistent kernel as job slots and frontier memory free up."""
     import torch
 
     import e13b200 as E
