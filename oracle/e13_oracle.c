@@ -18,8 +18,10 @@
  *                    sim_init :123-129, run :134-177, sym_next :206-212,
  *                    explore :214-254, setup :317-355, set_sym :423-426,
  *                    run_full :428-433, report :184-200
+ *   src/e13search.c  probe :256-313, estimate :473-510 (Knuth size estimate)
  *   src/recheck.c    main :22-103   (exact counter sets per stage)
  *   src/deep.c       main :15-84    (counter size and leftmost one per stage)
+ *   src/check.py     :1-173         (stages to 11, crafted stage starts, its text)
  *
  * The structure is this file's own: the DFS keeps whole machine snapshots in
  * its frontier (no replay from the blank tape), and the parallel phase is a
