@@ -296,10 +296,11 @@ __device__ __forceinline__ u64 counter_hash(const u32 *tcol, const u64 *keyc, in
 // The stage-start test of src/e13search.c:136-161 once hb matches TGT[nt].
 // Returns 0 (go on), kEvDead or kEvSurv.
 __device__ __forceinline__ int stage_check(Lane &L, const u32 *tcol, const u64 *keyc, int stride) {
-  const int nt = L.nt, c = s_exc[nt];
+  const int nt = L.nt;
+  if (nt > 1 && L.st != L.st0) return 0;  // the common rejection, before any load
+  const int c = s_exc[nt];
   int a = L.flags & kFlagAbs, r = (L.flags >> 1) & 1;
   if (nt > 1) {
-    if (L.st != L.st0) return 0;
     if (L.p != L.p0) a = 0;
     if (L.p - (1 << nt) != L.p0 - 2) r = 0;
     if (!a && !r) return 0;
