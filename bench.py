@@ -247,7 +247,7 @@ def serving_bench(args, w, ws, rank, local, pg):
         jobs.append(job)
         arrivals.append(t)
     ctx = E.Context(local)
-    lat, steps, dev_ms, wall, leaves, epochs = [], 0, 0.0, 0.0, [], 0
+    lat, steps, dev_ms, wall, leaves, epochs, launches = [], 0, 0.0, 0.0, [], 0, 0
     for it in range(args.warmup + args.steps):
         with E.Server(ctx) as srv:
             t0 = time.perf_counter()
@@ -258,6 +258,7 @@ def serving_bench(args, w, ws, rank, local, pg):
             wall += dt
             dev_ms += ms
             epochs += ep
+            launches += ctx.stats().launches
             for r, surv in got.values():
                 steps += r.counts.steps
                 lat.append(r.t_done - r.t_submit)
@@ -270,7 +271,7 @@ def serving_bench(args, w, ws, rank, local, pg):
             "config": {"workload": f"serving_mix: {w['desc']}", "kernel": "persistent (serve)",
                        "jobs": len(jobs), "leaves_min": min(leaves), "leaves_max": max(leaves)},
             "latency_p50_s": p(0.50), "latency_p99_s": p(0.99),
-            "device_busy_frac": dev_ms / 1000 / wall, "gpu_launches": 4 * epochs,
+            "device_busy_frac": dev_ms / 1000 / wall, "gpu_launches": launches,
             "note": "value = steps of all jobs / wall time from the first arrival to the last completion; "
                     "jobs arrive on the host clock, so idle gaps between arrivals count"}
     print(json.dumps(line), flush=True)
@@ -335,7 +336,7 @@ def main():
                 leaves += r.counts.leaves
                 surv_bytes += 64 * len(surv)
             dev_ms = ms
-            launches = 4 * epochs  # search kernel, move, finish, per-job node count
+            launches = ctx.stats().launches  # search, move, finish, node count per epoch; frontier order
             kstats["epochs"] += epochs
         else:
             for job in jobs:

@@ -531,6 +531,23 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   }
 }
 
+// Serving: moves the frontier into dst grouped by job, job k's nodes starting
+// at fill[k] (the host lays the groups out so that the job with the fewest
+// live nodes ends on top, where the next epoch takes its input first).  One
+// warp per node.
+__global__ void order_by_job(const Ctl *ctl, const Node *src, Node *dst, unsigned long long *fill, long long cap) {
+  const long long top = ctl->top;
+  const int lane = threadIdx.x & 31;
+  const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long i = w0; i < top; i += nw) {
+    unsigned long long pos = 0;
+    if (lane == 0) pos = atomicAdd(&fill[src[i].job & (kMaxJobs - 1)], 1ull);
+    pos = __shfl_sync(kFull, pos, 0);
+    if ((long long)pos < cap) copy_node(dst + pos, src + i, lane);
+  }
+}
+
 // Live nodes of each job on the frontier stack.  Between launches every
 // unfinished machine of the persistent kernel is there, so a job whose count
 // is zero is finished.
@@ -1338,6 +1355,16 @@ struct e13_serve {
   double t0;
   double device_ms;
   long long epochs;
+  // frontier order between epochs: a second stack buffer, the group starts
+  Node *alt = nullptr;
+  long long alt_cap = 0;
+  unsigned long long *d_fill = nullptr;
+  unsigned long long fill[kMaxJobs];
+  bool reorder = false;
+  ~e13_serve() {
+    cudaFree(alt);
+    cudaFree(d_fill);
+  }
 };
 
 extern "C" int e13_serve_create(e13_ctx *c, const e13_tuning *tuning, int64_t reserve_nodes, e13_serve **out) {
@@ -1345,7 +1372,7 @@ extern "C" int e13_serve_create(e13_ctx *c, const e13_tuning *tuning, int64_t re
   *out = nullptr;
   e13_tuning tu;
   e13_default_tuning(&tu);
-  tu.epoch_us = 20000;  // short epochs: new jobs join at every epoch boundary
+  tu.epoch_us = 10000;  // short epochs: new jobs join, and finished ones leave, at every epoch boundary
   if (tuning) {
     if (tuning->block) tu.block = tuning->block;
     if (tuning->slice) tu.slice = tuning->slice;
@@ -1406,7 +1433,11 @@ extern "C" int e13_serve_create(e13_ctx *c, const e13_tuning *tuning, int64_t re
   CK(cudaMemsetAsync(c->pool_ready, 0, sizeof(int) * (size_t)c->pool_ready_cap, c->stream));
   CK(cudaMemsetAsync(c->d_jobcnt, 0, sizeof(unsigned long long) * kMaxJobs * kJobCounters, c->stream));
   CK(cudaMemcpyAsync(c->d_jobs, s->jp, sizeof s->jp, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMalloc(&s->alt, sizeof(Node) * (size_t)c->stack_cap));
+  s->alt_cap = c->stack_cap;
+  CK(cudaMalloc(&s->d_fill, sizeof(unsigned long long) * kMaxJobs));
   CK(cudaStreamSynchronize(c->stream));
+  memset(&c->stats, 0, sizeof c->stats);
   s->t0 = wall_seconds();
   *out = s.release();
   return E13_OK;
@@ -1445,6 +1476,18 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
   e13_ctx *c = s->c;
   CK(cudaSetDevice(c->device));
   const double now = e13_serve_clock(s);
+  CK(cudaEventRecord(c->k0, c->stream));
+  long long launches = 0;
+  // 0. the frontier in the order the last step chose (fewest live nodes on top)
+  if (s->reorder && s->alt_cap >= c->stack_cap) {
+    CK(cudaMemcpyAsync(s->d_fill, s->fill, sizeof s->fill, cudaMemcpyHostToDevice, c->stream));
+    order_by_job<<<c->nsm * 4, 256, 0, c->stream>>>(c->ctl, c->stack, s->alt, s->d_fill, s->alt_cap);
+    CK(cudaGetLastError());
+    std::swap(c->stack, s->alt);
+    s->P.stack = c->stack;
+    ++launches;
+  }
+  s->reorder = false;
   // 1. admission: a free slot, the job's arrival time passed, and frontier room
   //    for every running job's reservation plus this one
   int running = 0;
@@ -1483,7 +1526,7 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
   }
   if (running == 0) return E13_OK;
   // 2. one epoch of the persistent kernel, then the live nodes of every job
-  CK(cudaEventRecord(c->k0, c->stream));
+  launches += 4;
   search_kernel<true><<<c->nsm, s->tu.block, s->smem, c->stream>>>(s->P);
   move_outputs<<<c->nsm * 4, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, c->stack_cap);
   finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, s->batch_max, c->pool_cap);
@@ -1501,6 +1544,10 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
   cudaEventElapsedTime(&ms, c->k0, c->k1);
   s->device_ms += ms;
   s->epochs += 1;
+  c->stats.device_ms += ms;
+  c->stats.launches += launches;
+  c->stats.search_kernel_launches += 1;
+  c->stats.epochs += 1;
   if (c->ctl_host->error) return (c->ctl_host->error & kErrTimeout) ? E13_ERR_TIMEOUT : E13_ERR_OVERFLOW;
   // 3. survivors found in this epoch go to their jobs
   const unsigned long long ns = c->ctl_host->nsurv;
@@ -1539,7 +1586,29 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
     s->finished_surv[j.id] = std::move(j.surv);
     s->slot_job[k].reset();
   }
-  // 5. idle: start the survivor buffer over
+  // 5. the order of the frontier for the next epoch, which takes its input
+  //    from the top: the job with the most live nodes at the bottom, the one
+  //    with the fewest on top (nearly finished jobs finish first); on a tie the
+  //    job started later goes higher.  Only when every node is accounted for.
+  {
+    int order[kMaxJobs], n = 0;
+    for (int k = 0; k < kMaxJobs; ++k)
+      if (s->slot_job[k] && nodes[k] > 0) order[n++] = k;
+    if (n > 1) {
+      std::sort(order, order + n, [&](int a, int b) {
+        if (nodes[a] != nodes[b]) return nodes[a] > nodes[b];
+        return s->slot_job[a]->t_start < s->slot_job[b]->t_start;
+      });
+      unsigned long long off = 0;
+      memset(s->fill, 0, sizeof s->fill);
+      for (int i = 0; i < n; ++i) {
+        s->fill[order[i]] = off;
+        off += nodes[order[i]];
+      }
+      s->reorder = off == (unsigned long long)c->ctl_host->top;
+    }
+  }
+  // 6. idle: start the survivor buffer over
   if (e13_serve_pending(s) == 0) {
     unsigned long long zero = 0;
     CK(cudaMemcpyAsync(&c->ctl->nsurv, &zero, sizeof zero, cudaMemcpyHostToDevice, c->stream));

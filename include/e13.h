@@ -223,7 +223,7 @@ int e13_estimate(e13_ctx *ctx, const e13_job *job, int64_t probes, uint64_t seed
    passed and the frontier stack has room for every running job's reservation
    (reserve_nodes, 0 = 64 Ki nodes) plus its own; the serve stack holds
    tuning->stack_nodes nodes (0 = 16 Mi nodes, 5 GB).  e13_serve_step admits,
-   runs one epoch (tuning->epoch_us, default 20 ms) and returns the jobs that
+   runs one epoch (tuning->epoch_us, default 10 ms) and returns the jobs that
    finished in it: a job is finished when none of its nodes is left on the
    frontier.  Each job's counts equal those of e13_search on that job alone.
    A context runs one serve session at a time and no e13_search meanwhile. */
