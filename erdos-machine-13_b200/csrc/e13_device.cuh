@@ -334,7 +334,7 @@ __device__ __forceinline__ u32 get_entry(const u32 *rcol, int stride, int cell) 
 
 // The 16-bit slot of a cell holding entry v, with the self-loop bit when
 // run_skip is on and v is a read move that keeps the state and the symbol.
-__device__ __forceinline__ u32 cell_slot(int cell, u32 v, bool run_skip) {
+__host__ __device__ __forceinline__ u32 cell_slot(int cell, u32 v, bool run_skip) {
   const bool self = run_skip && v < 64u && (int)(v >> 2) == (cell >> 1) && (int)(v & 1u) == (cell & 1);
   return v | (self ? kEntSelf : 0u);
 }
@@ -343,6 +343,25 @@ __device__ __forceinline__ void set_entry(u32 *rcol, int stride, int cell, u32 v
   u32 *w = rcol + (cell >> 1) * stride;
   const int sh = (cell & 1) << 4;
   *w = (*w & ~(0xFFFFu << sh)) | (cell_slot(cell, v, run_skip) << sh);
+}
+
+// With no budget left, a first read of a cell that is not free can only keep
+// the table's move (src/e13search.c:221-251 with budget 0: the keep child
+// alone).  Clearing the unread flag of every such cell lets the step loop
+// take those reads as plain steps instead of events.  Unread halts keep the
+// flag (their read ends the machine), free cells keep theirs (they fork).
+// The flag also marks the survivor's never-read cells ('?'), so survivors are
+// given their read mask again by survivor_read_masks().  An unread move's
+// slot carries its self-loop bit already (see build_root), so clearing bit 7
+// is all it takes.
+static __device__ __noinline__ void clear_unread(u32 *rcol, int stride) {
+#pragma unroll 1
+  for (int s = 0; s < 16; ++s) {
+    const u32 w = rcol[s * stride];
+    // bit 7 set and bit 6 clear in a slot: an unread move (codes are < 64)
+    const u32 unread_move = (w & 0x00800080u) & ~((w & 0x00400040u) << 1);
+    rcol[s * stride] = w & ~unread_move;
+  }
 }
 
 // Relabel symmetry (src/e13search.c:206-212): states in use after move v, or

@@ -77,15 +77,21 @@ __device__ __forceinline__ void lane_store(const Lane &L, Node *N, const u32 *tc
 
 // Applies child `ch` (-1: keep / go on, else move v) of node N to a lane that
 // has just loaded N.
+// clear: on the move that spends the last of the budget, clear the unread
+// flags that can no longer fork (clear_unread; the search, not the estimator,
+// which counts every first read as a fork).
 __device__ __forceinline__ void apply_child(Lane &L, const Node *N, int ch, u32 *rcol, int stride, int sym_lo,
-                                            int sym_hi, bool run_skip) {
+                                            int sym_hi, bool run_skip, bool clear = false) {
   const int pend = N->pend;
   if (pend < 0) return;
   const u32 e = N->cellv[pend] & 0xFFu;
   if (ch < 0) {
     set_entry(rcol, stride, pend, e & 0x7Fu, run_skip);  // the table's own move (or halt), now read
   } else {
-    if (e != kEntFree) L.budget -= 1;
+    if (e != kEntFree) {
+      L.budget -= 1;
+      if (clear && L.budget == 0) clear_unread(rcol, stride);
+    }
     L.nintro = sym_after(ch, L.nintro, sym_lo, sym_hi);
     set_entry(rcol, stride, pend, (u32)ch, run_skip);
   }
@@ -94,8 +100,11 @@ __device__ __forceinline__ void apply_child(Lane &L, const Node *N, int ch, u32 
 // ------------------------------------------------------------------------
 // host side
 
-// The root of a job: blank tape, every cell unread (free cells: kEntFree).
-static inline void build_root(const e13_job *job, int slot, Node *root) {
+// The root of a job: blank tape, every cell unread (free cells: kEntFree).  An
+// unread move carries its self-loop bit (when run_skip is on) for the moment
+// its flag is cleared.  clear: a job with no budget starts with the flags of
+// its moves cleared (clear_unread).
+static inline void build_root(const e13_job *job, int slot, Node *root, bool run_skip = false, bool clear = false) {
   memset(root, 0, sizeof *root);
   root->job = (unsigned char)slot;
   root->p = kLeft;
@@ -113,9 +122,9 @@ static inline void build_root(const e13_job *job, int slot, Node *root) {
       const int c = job->tab[i];
       if (c == E13_FREE) e = (unsigned char)kEntFree;
       else if (c < 0) e = (unsigned char)(kEntUnread | kEntHalt);
-      else e = (unsigned char)(kEntUnread | (unsigned)c);
+      else e = (unsigned char)(((clear && job->budget <= 0) ? 0u : kEntUnread) | (unsigned)c);
     }
-    root->cellv[i] = e;
+    root->cellv[i] = (unsigned short)(e < 64u || (e & 0xC0u) == kEntUnread ? cell_slot(i, e & 0x3Fu, run_skip) | (e & kEntUnread) : e);
   }
 }
 

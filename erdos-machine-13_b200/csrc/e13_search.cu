@@ -227,7 +227,10 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
           if (first < 0) {
             set_entry(rcol, stride, fork_cell, fork_e & 0x7Fu, P.run_skip);
           } else {
-            if (fork_e != kEntFree) L.budget -= 1;
+            if (fork_e != kEntFree) {
+              L.budget -= 1;
+              if (L.budget == 0) clear_unread(rcol, stride);  // no first read can fork any more
+            }
             L.nintro = sym_after(first, L.nintro, s_jp[L.job].y, s_jp[L.job].z);
             set_entry(rcol, stride, fork_cell, (u32)first, P.run_skip);
           }
@@ -353,7 +356,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
         if (!(cur_keep && rank == 0)) ch = nth_bit64(cur_vm, rank - cur_keep);
         if (N->job != L.job) flush_counts();
         lane_load(L, N, tcol, rcol, stride, P.nq);
-        apply_child(L, N, ch, rcol, stride, s_jp[N->job].y, s_jp[N->job].z, P.run_skip);
+        apply_child(L, N, ch, rcol, stride, s_jp[N->job].y, s_jp[N->job].z, P.run_skip, true);
         status = kStRun;
       }
       __syncwarp();
@@ -545,6 +548,37 @@ __global__ void order_by_job(const Ctl *ctl, const Node *src, Node *dst, unsigne
     if (lane == 0) pos = atomicAdd(&fill[src[i].job & (kMaxJobs - 1)], 1ull);
     pos = __shfl_sync(kFull, pos, 0);
     if ((long long)pos < cap) copy_node(dst + pos, src + i, lane);
+  }
+}
+
+// The read mask of survivors [from, to): cells whose unread flag was cleared
+// when their machine's budget ran out (clear_unread) look read in the record.
+// A survivor's run is fixed by its final table, so running that table from the
+// blank tape for its t steps reads exactly the cells its search run read
+// (src/e13search.c:186-196 prints the others with '?').  Those get the unread
+// flag back; every cell read loses it.  One thread per survivor.
+__global__ void survivor_read_masks(SurvRec *recs, long long from, long long to) {
+  const long long i = from + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= to) return;
+  SurvRec &r = recs[i];
+  u32 tape[kTapeWords];
+  for (int w = 0; w < kTapeWords; ++w) tape[w] = 0;
+  int p = kLeft, st = 0;
+  u32 read = 0;
+  for (int t = 0; t < r.t; ++t) {
+    const int sym = (int)((tape[p >> 5] >> (p & 31)) & 1u);
+    const int cell = 2 * st + sym;
+    read |= 1u << cell;
+    const u32 e = r.ent[cell];
+    if (e == kEntFree || (e & kEntHalt)) break;  // a survivor reads neither before its end
+    if ((e & 1u) != (u32)sym) tape[p >> 5] ^= 1u << (p & 31);
+    p += (e & 2u) ? 1 : -1;
+    if (p < 1 || p > kTapeCells - 2) break;     // nor leaves the window
+    st = (int)((e >> 2) & 15u);
+  }
+  for (int c = 0; c < 32; ++c) {
+    const u32 e = r.ent[c];
+    if (e != kEntFree) r.ent[c] = (unsigned char)(((read >> c) & 1u) ? (e & 0x7Fu) : (e | kEntUnread));
   }
 }
 
@@ -1091,7 +1125,7 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
 
   // the root: blank tape, every cell unread
   Node root;
-  build_root(job, 0, &root);
+  build_root(job, 0, &root, tu.run_skip != 0, true);
   memset(c->ctl_host, 0, sizeof(Ctl));
   c->ctl_host->top = 1;
   c->ctl_host->batch = 1;
@@ -1217,7 +1251,10 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
   const long long ncopy = std::min<long long>(ns, std::min<long long>(surv_cap, c->surv_cap));
   if (ncopy > 0) {
     std::vector<SurvRec> recs((size_t)ncopy);
-    CK(cudaMemcpy(recs.data(), c->surv, sizeof(SurvRec) * (size_t)ncopy, cudaMemcpyDeviceToHost));
+    survivor_read_masks<<<(unsigned)((ncopy + 63) / 64), 64, 0, c->stream>>>(c->surv, 0, ncopy);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(recs.data(), c->surv, sizeof(SurvRec) * (size_t)ncopy, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     for (long long i = 0; i < ncopy; ++i) decode_survivor(recs[(size_t)i], job->nq, &surv[i]);
   }
   if (wall_s) *wall_s = prior_wall + (host_seconds() - t_call);
@@ -1509,7 +1546,7 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
     s->jp[slot].sym_lo = j->job.sym_lo;
     s->jp[slot].sym_hi = j->job.sym_hi;
     Node root;
-    build_root(&j->job, slot, &root);
+    build_root(&j->job, slot, &root, s->tu.run_skip != 0, true);
     roots.push_back(root);
     CK(cudaMemsetAsync(c->d_jobcnt + (size_t)slot * kJobCounters, 0, sizeof(unsigned long long) * kJobCounters,
                        c->stream));
@@ -1555,7 +1592,12 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
   if (ns > (unsigned long long)c->surv_cap) s->surv_overflow = true;
   if (avail > s->surv_fetched) {
     std::vector<SurvRec> recs((size_t)(avail - s->surv_fetched));
-    CK(cudaMemcpy(recs.data(), c->surv + s->surv_fetched, sizeof(SurvRec) * recs.size(), cudaMemcpyDeviceToHost));
+    survivor_read_masks<<<(unsigned)((recs.size() + 63) / 64), 64, 0, c->stream>>>(c->surv, (long long)s->surv_fetched,
+                                                                                   (long long)avail);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(recs.data(), c->surv + s->surv_fetched, sizeof(SurvRec) * recs.size(), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     for (const SurvRec &r : recs) {
       ServeJob *j = (r.job >= 0 && r.job < kMaxJobs) ? s->slot_job[r.job].get() : nullptr;
       if (!j) continue;
