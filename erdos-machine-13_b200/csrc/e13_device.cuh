@@ -351,7 +351,7 @@ __device__ __forceinline__ void set_entry(u32 *rcol, int stride, int cell, u32 v
 // take those reads as plain steps instead of events.  Unread halts keep the
 // flag (their read ends the machine), free cells keep theirs (they fork).
 // The flag also marks the survivor's never-read cells ('?'), so survivors are
-// given their read mask again by survivor_read_masks().  An unread move's
+// given their read mask again at survival (survivor_reads).  An unread move's
 // slot carries its self-loop bit already (see build_root), so clearing bit 7
 // is all it takes.
 static __device__ __noinline__ void clear_unread(u32 *rcol, int stride) {

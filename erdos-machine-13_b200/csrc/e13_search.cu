@@ -71,18 +71,53 @@ __device__ __forceinline__ void copy_node(Node *dst, const Node *src, int lane) 
   if (lane < kNodeChunks) reinterpret_cast<uint4 *>(dst)[lane] = reinterpret_cast<const uint4 *>(src)[lane];
 }
 
-__device__ __forceinline__ void record_survivor(const Params &P, const Lane &L, const u32 *rcol, int stride) {
-  const unsigned long long k = atomicAdd(&P.ctl->nsurv, 1ull);
-  if ((long long)k >= P.surv_cap) return;
-  SurvRec *r = P.surv + k;
-  u32 *e32 = reinterpret_cast<u32 *>(r->ent);
-  for (int k2 = 0; k2 < 8; ++k2) e32[k2] = __byte_perm(rcol[(2 * k2) * stride], rcol[(2 * k2 + 1) * stride], 0x6420);
-  r->st0 = L.st0;
-  r->head0 = L.p0 - kLeft;
-  r->abs_ok = L.flags & 1;
-  r->rel_ok = (L.flags >> 1) & 1;
-  r->t = L.t;
-  r->job = L.job;
+// The cells a survivor's run read.  Unread flags cleared when the budget ran
+// out (clear_unread) make some never-read cells look read, so the lane runs
+// its final table again from the blank tape, in its own tape, for the t steps
+// of its run: a run is fixed by its table, so this reads exactly the cells the
+// search run read (the reference prints the others with '?',
+// src/e13search.c:186-196).  Survivors are rare; the lane is idle afterwards,
+// and its next load clears the tape words of t steps, the ones used here.
+static __device__ __noinline__ u32 survivor_reads(u32 *tcol, const u32 *rcol, int stride, int t) {
+  int lo, hi;
+  tape_extent(t, lo, hi);
+  for (int w = lo; w <= hi; ++w) tcol[w * stride] = 0;
+  int p = kLeft, st = 0;
+  u32 read = 0;
+  for (int k = 0; k < t; ++k) {
+    const int widx = (p >> 5) * stride;
+    const u32 word = tcol[widx];
+    const u32 sym = (word >> (p & 31)) & 1u;
+    read |= 1u << (2 * st + (int)sym);
+    const u32 e = (rcol[st * stride] >> (sym << 4)) & 0xFFu;
+    if (e == kEntFree || (e & kEntHalt)) break;  // a survivor reads neither before its end
+    tcol[widx] = word ^ (((e ^ sym) & 1u) << (p & 31));
+    p += (e & 2u) ? 1 : -1;
+    if (p < 1 || p > kTapeCells - 2) break;     // nor leaves the window
+    st = (int)((e >> 2) & 15u);
+  }
+  return read;
+}
+
+// Appends a survivor record (kept only below the cap).  Out of line: it is
+// rare, and the step loop keeps its registers.
+static __device__ __noinline__ void record_survivor(Ctl *ctl, SurvRec *surv, long long surv_cap, int st0, int p0,
+                                                    int flags, int t, int job, u32 *tcol, const u32 *rcol,
+                                                    int stride) {
+  const unsigned long long k = atomicAdd(&ctl->nsurv, 1ull);
+  if ((long long)k >= surv_cap) return;
+  SurvRec *r = surv + k;
+  const u32 read = survivor_reads(tcol, rcol, stride, t);
+  for (int c = 0; c < 32; ++c) {
+    const u32 e = (rcol[(c >> 1) * stride] >> ((c & 1) << 4)) & 0xFFu;
+    r->ent[c] = (unsigned char)(e == kEntFree ? e : (((read >> c) & 1u) ? (e & 0x7Fu) : (e | kEntUnread)));
+  }
+  r->st0 = st0;
+  r->head0 = p0 - kLeft;
+  r->abs_ok = flags & 1;
+  r->rel_ok = (flags >> 1) & 1;
+  r->t = t;
+  r->job = job;
 }
 
 enum { kStRun = 0, kStIdle = 1, kStFork = 2, kStCap = 3 };
@@ -499,7 +534,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
               ++acc_leaves;
               if (acc_steps >= 0x80000000u) flush_counts();
               if (ev == kEvDead) atomicAdd(&s_jc[L.job][2 + L.stage], 1ull);
-              else record_survivor(P, L, rcol, stride);
+              else record_survivor(P.ctl, P.surv, P.surv_cap, L.st0, L.p0, L.flags, L.t, L.job, tcol, rcol, stride);
               status = kStIdle;
             }
           }
@@ -548,37 +583,6 @@ __global__ void order_by_job(const Ctl *ctl, const Node *src, Node *dst, unsigne
     if (lane == 0) pos = atomicAdd(&fill[src[i].job & (kMaxJobs - 1)], 1ull);
     pos = __shfl_sync(kFull, pos, 0);
     if ((long long)pos < cap) copy_node(dst + pos, src + i, lane);
-  }
-}
-
-// The read mask of survivors [from, to): cells whose unread flag was cleared
-// when their machine's budget ran out (clear_unread) look read in the record.
-// A survivor's run is fixed by its final table, so running that table from the
-// blank tape for its t steps reads exactly the cells its search run read
-// (src/e13search.c:186-196 prints the others with '?').  Those get the unread
-// flag back; every cell read loses it.  One thread per survivor.
-__global__ void survivor_read_masks(SurvRec *recs, long long from, long long to) {
-  const long long i = from + (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= to) return;
-  SurvRec &r = recs[i];
-  u32 tape[kTapeWords];
-  for (int w = 0; w < kTapeWords; ++w) tape[w] = 0;
-  int p = kLeft, st = 0;
-  u32 read = 0;
-  for (int t = 0; t < r.t; ++t) {
-    const int sym = (int)((tape[p >> 5] >> (p & 31)) & 1u);
-    const int cell = 2 * st + sym;
-    read |= 1u << cell;
-    const u32 e = r.ent[cell];
-    if (e == kEntFree || (e & kEntHalt)) break;  // a survivor reads neither before its end
-    if ((e & 1u) != (u32)sym) tape[p >> 5] ^= 1u << (p & 31);
-    p += (e & 2u) ? 1 : -1;
-    if (p < 1 || p > kTapeCells - 2) break;     // nor leaves the window
-    st = (int)((e >> 2) & 15u);
-  }
-  for (int c = 0; c < 32; ++c) {
-    const u32 e = r.ent[c];
-    if (e != kEntFree) r.ent[c] = (unsigned char)(((read >> c) & 1u) ? (e & 0x7Fu) : (e | kEntUnread));
   }
 }
 
@@ -1251,8 +1255,6 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
   const long long ncopy = std::min<long long>(ns, std::min<long long>(surv_cap, c->surv_cap));
   if (ncopy > 0) {
     std::vector<SurvRec> recs((size_t)ncopy);
-    survivor_read_masks<<<(unsigned)((ncopy + 63) / 64), 64, 0, c->stream>>>(c->surv, 0, ncopy);
-    CK(cudaGetLastError());
     CK(cudaMemcpyAsync(recs.data(), c->surv, sizeof(SurvRec) * (size_t)ncopy, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     for (long long i = 0; i < ncopy; ++i) decode_survivor(recs[(size_t)i], job->nq, &surv[i]);
@@ -1592,9 +1594,6 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
   if (ns > (unsigned long long)c->surv_cap) s->surv_overflow = true;
   if (avail > s->surv_fetched) {
     std::vector<SurvRec> recs((size_t)(avail - s->surv_fetched));
-    survivor_read_masks<<<(unsigned)((recs.size() + 63) / 64), 64, 0, c->stream>>>(c->surv, (long long)s->surv_fetched,
-                                                                                   (long long)avail);
-    CK(cudaGetLastError());
     CK(cudaMemcpyAsync(recs.data(), c->surv + s->surv_fetched, sizeof(SurvRec) * recs.size(), cudaMemcpyDeviceToHost,
                        c->stream));
     CK(cudaStreamSynchronize(c->stream));
