@@ -94,7 +94,7 @@ def serving_mix(seed=2026, n=40, rate=25.0):
 # DRAM bytes (read + write) of one 200 ms epoch launch of the persistent search
 # kernel, from the ncu capture summarised in
 # profiles/search_kernel_persistent_local_edits_f4.md
-PROFILED_TRAFFIC = {"local_edits_f4": 434.6e6}
+PROFILED_TRAFFIC = {"local_edits_f4": 386.7e6}
 OPS_PER_STEP = 16  # integer lane-ops per simulated step (hash test 2, deadline 1, address 1, load+extract 2,
 #                    index 1, table 2, fork test 1, halt test 1, write test 1, head 2, bounds 2)
 
