@@ -99,18 +99,23 @@ static __device__ __noinline__ u32 survivor_reads(u32 *tcol, const u32 *rcol, in
   return read;
 }
 
-// Appends a survivor record (kept only below the cap).  Out of line: it is
-// rare, and the step loop keeps its registers.
+// Appends a survivor record (kept only below the cap).  reads: the persistent
+// kernel has the lane re-run the table for the read mask (its warp goes on
+// alone, the others are not held up); the plain kernel, whose launch would
+// wait for that lane, records the flags as they are and leaves the mask to
+// survivor_read_masks() once the search is over.  Out of line: it is rare, and
+// the step loop keeps its registers.
 static __device__ __noinline__ void record_survivor(Ctl *ctl, SurvRec *surv, long long surv_cap, int st0, int p0,
                                                     int flags, int t, int job, u32 *tcol, const u32 *rcol,
-                                                    int stride) {
+                                                    int stride, bool reads) {
   const unsigned long long k = atomicAdd(&ctl->nsurv, 1ull);
   if ((long long)k >= surv_cap) return;
   SurvRec *r = surv + k;
-  const u32 read = survivor_reads(tcol, rcol, stride, t);
+  const u32 read = reads ? survivor_reads(tcol, rcol, stride, t) : 0u;
   for (int c = 0; c < 32; ++c) {
     const u32 e = (rcol[(c >> 1) * stride] >> ((c & 1) << 4)) & 0xFFu;
-    r->ent[c] = (unsigned char)(e == kEntFree ? e : (((read >> c) & 1u) ? (e & 0x7Fu) : (e | kEntUnread)));
+    if (!reads) r->ent[c] = (unsigned char)e;
+    else r->ent[c] = (unsigned char)(e == kEntFree ? e : (((read >> c) & 1u) ? (e & 0x7Fu) : (e | kEntUnread)));
   }
   r->st0 = st0;
   r->head0 = p0 - kLeft;
@@ -534,7 +539,8 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
               ++acc_leaves;
               if (acc_steps >= 0x80000000u) flush_counts();
               if (ev == kEvDead) atomicAdd(&s_jc[L.job][2 + L.stage], 1ull);
-              else record_survivor(P.ctl, P.surv, P.surv_cap, L.st0, L.p0, L.flags, L.t, L.job, tcol, rcol, stride);
+              else record_survivor(P.ctl, P.surv, P.surv_cap, L.st0, L.p0, L.flags, L.t, L.job, tcol, rcol, stride,
+                                   PERSIST);
               status = kStIdle;
             }
           }
@@ -583,6 +589,36 @@ __global__ void order_by_job(const Ctl *ctl, const Node *src, Node *dst, unsigne
     if (lane == 0) pos = atomicAdd(&fill[src[i].job & (kMaxJobs - 1)], 1ull);
     pos = __shfl_sync(kFull, pos, 0);
     if ((long long)pos < cap) copy_node(dst + pos, src + i, lane);
+  }
+}
+
+// The read masks of survivors [0, n) recorded by the plain kernel: the same
+// re-run as survivor_reads(), one thread per survivor, once the search is
+// over (every survivor in parallel, instead of holding up a launch each).
+__global__ void survivor_read_masks(SurvRec *recs, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  SurvRec &r = recs[i];
+  unsigned char ent[32];
+  for (int c = 0; c < 32; ++c) ent[c] = r.ent[c];
+  u32 tape[kTapeWords];
+  for (int w = 0; w < kTapeWords; ++w) tape[w] = 0;
+  int p = kLeft, st = 0;
+  u32 read = 0;
+  for (int k = 0; k < r.t; ++k) {
+    const u32 sym = (tape[p >> 5] >> (p & 31)) & 1u;
+    const int cell = 2 * st + (int)sym;
+    read |= 1u << cell;
+    const u32 e = ent[cell];
+    if (e == kEntFree || (e & kEntHalt)) break;  // a survivor reads neither before its end
+    tape[p >> 5] ^= ((e ^ sym) & 1u) << (p & 31);
+    p += (e & 2u) ? 1 : -1;
+    if (p < 1 || p > kTapeCells - 2) break;     // nor leaves the window
+    st = (int)((e >> 2) & 15u);
+  }
+  for (int c = 0; c < 32; ++c) {
+    const u32 e = ent[c];
+    if (e != kEntFree) r.ent[c] = (unsigned char)(((read >> c) & 1u) ? (e & 0x7Fu) : (e | kEntUnread));
   }
 }
 
@@ -1255,6 +1291,10 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
   const long long ncopy = std::min<long long>(ns, std::min<long long>(surv_cap, c->surv_cap));
   if (ncopy > 0) {
     std::vector<SurvRec> recs((size_t)ncopy);
+    if (!persist) {
+      survivor_read_masks<<<(unsigned)((ncopy + 31) / 32), 32, 0, c->stream>>>(c->surv, ncopy);
+      CK(cudaGetLastError());
+    }
     CK(cudaMemcpyAsync(recs.data(), c->surv, sizeof(SurvRec) * (size_t)ncopy, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     for (long long i = 0; i < ncopy; ++i) decode_survivor(recs[(size_t)i], job->nq, &surv[i]);
