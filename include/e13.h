@@ -222,10 +222,12 @@ int e13_estimate(e13_ctx *ctx, const e13_job *job, int64_t probes, uint64_t seed
    survivors.  A job is admitted when a slot is free, its submit time has
    passed and the frontier stack has room for every running job's reservation
    (reserve_nodes, 0 = 64 Ki nodes) plus its own; the serve stack holds
-   tuning->stack_nodes nodes (0 = 16 Mi nodes, 5 GB).  e13_serve_step admits,
-   runs one epoch (tuning->epoch_us, default 10 ms) and returns the jobs that
-   finished in it: a job is finished when none of its nodes is left on the
-   frontier.  Each job's counts equal those of e13_search on that job alone.
+   tuning->stack_nodes nodes (0 = 16 Mi nodes, 5 GB), and a second buffer of
+   the same size lets the frontier be regrouped between epochs, the job with
+   the fewest live nodes on top.  e13_serve_step admits, runs one epoch
+   (tuning->epoch_us, default 10 ms) and returns the jobs that finished in it:
+   a job is finished when none of its nodes is left on the frontier.  Each
+   job's counts equal those of e13_search on that job alone.
    A context runs one serve session at a time and no e13_search meanwhile. */
 typedef struct e13_serve e13_serve;
 typedef struct e13_serve_result {
