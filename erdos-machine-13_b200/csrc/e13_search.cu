@@ -13,11 +13,15 @@
 //    stack and goes on with the first child in place (no copy); idle lanes take
 //    the next children of the stack top at the next round.  A warp whose stack
 //    is deep donates its oldest node to a device pool when the pool runs low;
-//    warps without work take pool nodes.  An epoch ends on a time bound (or
-//    when every warp is out of work): warps then dump live lanes and stack
-//    nodes back to the frontier.  Epochs
+//    warps without work take pool nodes.  An epoch takes the whole frontier as
+//    its input and ends on a time bound (or when every warp is out of work):
+//    warps then dump live lanes and stack nodes back to the frontier.  Epochs
 //    are replayed from a captured CUDA graph; the host reads the control block
 //    once per graph.
+//
+// In both, a machine whose budget is spent takes first reads of cells that
+// can no longer fork as plain steps (clear_unread); survivors get their read
+// mask back from a re-run of their final table.
 //
 // Leaves, steps and deaths per stage are exact and equal the reference's
 // (src/e13search.c:214-254 explore, :357-420 run_delete).
