@@ -97,12 +97,19 @@ int e13_setup(const int32_t *base, int nq0, int X, int fmax, const uint8_t *free
     row++;
   }
   job->nforced = nF;
-  if (lo >= 0) {
-    int slo = lo - (lo > X), shi = hi - (hi >= X), n0 = 0;
+  /* symmetry is on only if the renumbered LO is >= 0 (src/e13search.c:336,
+     :424): with no deleted state (X = -1) LO..HI shift down by one, so LO = 0
+     turns it off */
+  const int slo = lo >= 0 ? lo - (lo > X) : -1, shi = lo >= 0 ? hi - (hi >= X) : -1;
+  if (slo >= 0) {
+    int n0 = 0;
     uint8_t named[E13_MAXQ + 1] = {0};
     job->sym_lo = slo;
     job->sym_hi = shi;
-    if (slo < 0 || shi >= job->nq || shi < slo) return E13_ERR_ARG;
+    /* an empty range (HI < LO after renumbering) is accepted and changes
+       nothing, as in the reference; one past the last state is refused (the
+       reference would read past its table there) */
+    if (shi >= job->nq) return E13_ERR_ARG;
     /* the reference scans the first 2*(NQ-1) cells, also when X < 0 */
     for (int i = 0; i < 2 * (nq0 - 1); i++) {
       int c = job->tab[i];

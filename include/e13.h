@@ -133,8 +133,11 @@ int e13_parse_machine(const char *text, int32_t base[E13_MAXCELLS]);
 
 /* Candidate construction (src/e13search.c:317-355 setup, :423-426 set_sym).
    free_cells: 2*nq0 flags in base numbering (NULL = delete mode with fmax).
-   lo < 0: no symmetry.  Returns E13_OK, E13_ERR_FMAX, E13_ERR_SYM_NAMED or
-   E13_ERR_SYM_START; job is filled as far as the reference gets. */
+   lo < 0: no symmetry.  LO..HI are renumbered as set_sym() does; a negative
+   renumbered LO (LO = 0 with X = -1) also means no symmetry, and an empty
+   range changes nothing, both as in the reference.  Returns E13_OK,
+   E13_ERR_FMAX, E13_ERR_SYM_NAMED or E13_ERR_SYM_START (E13_ERR_ARG for a
+   range past the last state); job is filled as far as the reference gets. */
 int e13_setup(const int32_t *base, int nq0, int X, int fmax, const uint8_t *free_cells, int lo, int hi,
               e13_job *job);
 

@@ -136,6 +136,13 @@ int oracle_setup(const int *base, int nq0, int X, int fmax, const unsigned char 
   if (lo >= 0) {
     slo = lo - (lo > X);
     shi = hi - (hi >= X);
+  }
+  /* symmetry is on only if the renumbered LO is >= 0 (e13search.c:336): with
+     no deleted state (X = -1) the reference shifts LO..HI down by one, so
+     LO = 0 turns it off */
+  if (slo < 0) {
+    slo = shi = -1;
+  } else {
     unsigned char named[O_MAXQ + 1] = {0};
     /* the reference scans 2*(NQ-1) cells even when X < 0 (e13search.c:341) */
     for (int i = 0; i < 2 * (nq0 - 1); i++) {

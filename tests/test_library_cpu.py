@@ -117,3 +117,34 @@ def test_resumable_search_checks_its_arguments():
                                   ctypes.byref(ns), None, None) == -1
     assert L.e13_search_resumable(None, ctypes.byref(job), None, None, ctypes.byref(counts), None, 0,
                                   ctypes.byref(ns), None, None) == -1
+
+
+def test_setup_random_free_sets_match_oracle():
+    """Candidate setup over 400 seeded random cases (machine, deleted state,
+    free set, symmetry range): the library's status, table and symmetry
+    fields equal the oracle's restatement of setup()/set_sym()."""
+    import random
+    rng = random.Random(13)
+    machines = ["erdos_14.txt", "split_15.txt", "c0_1RD.txt", "counters_3state/base_07.txt",
+                "counters_3state/base_33.txt"]
+    checked = 0
+    for _ in range(400):
+        base = O.load_machine(rng.choice(machines))
+        nq0 = len(base) // 2
+        X = rng.randrange(-1, nq0)
+        nq = nq0 - (1 if X >= 0 else 0)
+        cells = rng.sample(range(2 * nq0), rng.randrange(1, 7))
+        free = [chr(ord("A") + c // 2) + str(c % 2) for c in cells]
+        if rng.random() < 0.5:
+            lo = rng.randrange(0, nq)
+            hi = rng.randrange(lo, nq)
+        else:
+            lo = hi = -1
+        r, job = E.setup(base, X, free_cells=free, lo=lo, hi=hi)
+        ro, jo = O.setup(base, X, free_cells=free, lo=lo, hi=hi)
+        assert r == (0 if ro >= 0 else ro), (X, free, lo, hi, r, ro)
+        if r == 0:
+            assert list(job.tab)[: 2 * job.nq] == jo.tab
+            assert (job.sym_lo, job.sym_hi, job.sym_n0) == (jo.sym_lo, jo.sym_hi, jo.sym_n0)
+            checked += 1
+    assert checked > 50

@@ -137,6 +137,10 @@ REFBIN = os.path.join(O.REF_DIR, "e13search")
     ["freesym", "erdos_14.txt", "9", "3", "9", "H0", "H1", "I0", "I1"],
     ["delete", "counters_3state/base_05.txt", "1", "-1"],
     ["delete", "split_15.txt", "2", "3"],
+    # no deleted state: the reference shifts LO..HI down by one, so LO = 0 turns symmetry off
+    ["freesym", "erdos_14.txt", "-1", "0", "9", "G0", "H0", "B0"],
+    # an empty range after renumbering (7..6): accepted, no symmetry
+    ["freesym", "erdos_14.txt", "7", "7", "7", "H0", "H1"],
 ])
 def test_oracle_vs_reference_binary(args):
     mode = args[0]
