@@ -148,3 +148,72 @@ def test_setup_random_free_sets_match_oracle():
             assert (job.sym_lo, job.sym_hi, job.sym_n0) == (jo.sym_lo, jo.sym_hi, jo.sym_n0)
             checked += 1
     assert checked > 50
+
+
+def test_survivor_lines_random_match_oracle():
+    """e13_format_survivor against the oracle's restatement of report()
+    (src/e13search.c:184-200) on 500 seeded random records: any moves, halts,
+    free cells, read masks, heads and step counts."""
+    import random
+    rng = random.Random(7)
+    base = O.load_machine("erdos_14.txt")
+    for _ in range(500):
+        nq = rng.randrange(1, 16)
+        r, job = E.setup(base, rng.randrange(-1, 14), fmax=4)
+        job.nq = nq
+        tab = [rng.choice([E.E13_HALT, E.E13_FREE] + list(range(4 * nq))) for _ in range(2 * nq)]
+        s = E.Survivor()
+        for i, c in enumerate(tab):
+            s.tab[i] = c
+        s.read_mask = rng.getrandbits(2 * nq)
+        s.st0, s.head0 = rng.randrange(0, nq), rng.randrange(-60, 1200)
+        s.abs_ok, s.rel_ok = rng.randrange(2), rng.randrange(2)
+        s.steps = rng.randrange(0, 835521)
+        rec = dict(tab=tab, mask=s.read_mask, st0=s.st0, head0=s.head0, abs=s.abs_ok, rel=s.rel_ok, steps=s.steps)
+        assert E.survivor_line(job, s) == O.survivor_line(job.X, rec, nq)
+
+
+def test_machine_text_random_matches_oracle():
+    """e13_parse_machine against load()/parse_cell() (src/e13search.c:105-121)
+    on 300 seeded random machine texts with halts, odd spacing and blank lines."""
+    import random
+    rng = random.Random(11)
+    for _ in range(300):
+        nq = rng.randrange(1, 17)
+        lines = []
+        for q in range(nq):
+            cells = []
+            for a in range(2):
+                if rng.random() < 0.1:
+                    cells.append("---")
+                else:
+                    cells.append(f"{rng.randrange(2)}{rng.choice('LR')}{rng.randrange(16)}")
+            lines.append((" " * rng.randrange(3)).join(["", ""]) + cells[0] + " " * rng.randrange(1, 4) + cells[1])
+            if rng.random() < 0.1:
+                lines.append("")
+        text = "\n".join(lines) + "\n"
+        assert E.parse_machine(text) == O.parse_machine_text(text)
+
+
+def test_setup_random_delete_with_symmetry_matches_oracle():
+    """Delete mode with a symmetry range (the reference's estimate mode allows
+    it, src/e13search.c:478-480): 300 seeded random cases, status, table,
+    budget and symmetry fields against the oracle."""
+    import random
+    rng = random.Random(5)
+    machines = ["erdos_14.txt", "split_15.txt", "counters_3state/base_21.txt"]
+    for _ in range(300):
+        base = O.load_machine(rng.choice(machines))
+        nq0 = len(base) // 2
+        X = rng.randrange(-1, nq0)
+        nq = nq0 - (1 if X >= 0 else 0)
+        lo = rng.randrange(-1, nq)
+        hi = rng.randrange(max(lo, 0), nq)
+        fmax = rng.randrange(0, 5)
+        r, job = E.setup(base, X, fmax=fmax, lo=lo, hi=hi)
+        ro, jo = O.setup(base, X, fmax=fmax, lo=lo, hi=hi)
+        assert r == (0 if ro >= 0 else (-2 if ro == -1 else ro)), (X, lo, hi, fmax, r, ro)
+        if r == 0:
+            assert job.budget == ro
+            assert list(job.tab)[: 2 * job.nq] == jo.tab
+            assert (job.sym_lo, job.sym_hi, job.sym_n0) == (jo.sym_lo, jo.sym_hi, jo.sym_n0)
