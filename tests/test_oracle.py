@@ -240,3 +240,35 @@ def test_check_py_restatement_equals_shipped_outputs():
             assert got[1:] == verdicts, (f, line[:80])
             n += 1
     assert n == 164
+
+
+def _random_free_cases(n, seed):
+    """Seeded small free / freesym searches on erdos_14 and a counter base:
+    (args for the reference binary)."""
+    import random
+    rng = random.Random(seed)
+    out = []
+    while len(out) < n:
+        machine = rng.choice(["erdos_14.txt", "counters_3state/base_12.txt"])
+        nq0 = len(O.load_machine(machine)) // 2
+        X = rng.randrange(-1, nq0)
+        cells = sorted(rng.sample(range(2 * nq0), rng.randrange(2, 4)))
+        names = [chr(ord("A") + c // 2) + str(c % 2) for c in cells]
+        if rng.random() < 0.5:
+            lo = rng.randrange(1, nq0)
+            hi = rng.randrange(lo, nq0)
+            base = O.load_machine(machine)
+            if O.setup(base, X, free_cells=names, lo=lo, hi=hi)[0] < 0:
+                continue  # the reference exits 1 on these; the setup tests cover them
+            out.append(["freesym", machine, str(X), str(lo), str(hi)] + names)
+        else:
+            out.append(["free", machine, str(X)] + names)
+    return out
+
+
+@pytest.mark.skipif(not os.path.exists(REFBIN), reason="reference binaries not built here")
+@pytest.mark.parametrize("args", _random_free_cases(12, 2026))
+def test_oracle_vs_reference_binary_random(args):
+    """The oracle against the reference program on seeded random free-cell
+    searches: leaves, survivors, steps, deaths per stage, survivor lines."""
+    test_oracle_vs_reference_binary(args)
