@@ -272,3 +272,54 @@ def test_oracle_vs_reference_binary_random(args):
     """The oracle against the reference program on seeded random free-cell
     searches: leaves, survivors, steps, deaths per stage, survivor lines."""
     test_oracle_vs_reference_binary(args)
+
+
+def _mutants(n, seed):
+    """Seeded single-cell mutants of V1 and V2 survivor lines: a cell gets a
+    random move or a halt, a fixed cell may become a never-read free one."""
+    import random
+    rng = random.Random(seed)
+    src = [l.rstrip("\n") for l in gzip.open(os.path.join(GOLD, "surv", "division_v1_1RD.txt.gz"), "rt") if "table=" in l]
+    src += [l.rstrip("\n") for l in open(os.path.join(GOLD, "surv", "division_v2_fileorder.txt")) if "table=" in l]
+    out = []
+    for _ in range(n):
+        line = rng.choice(src)
+        head, table = line.split("table=")
+        rows = [r.split() for r in table.split("|")]
+        q = rng.randrange(len(rows))
+        a = rng.randrange(2)
+        u = rng.random()
+        if u < 0.15:
+            rows[q][a] = "---"
+        elif u < 0.25:
+            rows[q][a] = "?---"
+        else:
+            rows[q][a] = f"{rng.randrange(2)}{rng.choice('LR')}{rng.randrange(len(rows))}"
+        out.append(head + "table=" + "|".join(" ".join(r) for r in rows))
+    return out
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(O.REF_DIR, "recheck")), reason="reference binaries not built here")
+def test_recheck_and_deep_vs_reference_binaries_on_mutants():
+    """The oracle's recheck.c / deep.c restatements against the reference
+    programs on 60 seeded mutants of real survivors, which fail at every kind
+    of point (counter change, limit, off tape, halt, free cell read)."""
+    lines = _mutants(60, 31)
+    nmax = 11
+    data = "\n".join(lines) + "\n"
+    rr = subprocess.run([os.path.join(O.REF_DIR, "recheck"), str(nmax)], input=data, capture_output=True, text=True,
+                        check=True, timeout=600)
+    ref = [l.split(": ", 1)[1] for l in rr.stdout.splitlines() if ": " in l]
+    assert len(ref) == len(lines)
+    kinds = set()
+    for line, want in zip(lines, ref):
+        ok, got, _ = O.recheck_line(line, nmax)
+        assert got == want, (line, got, want)
+        kinds.add(want.split(" ")[0])
+    assert len(kinds) >= 3  # several verdict kinds were exercised
+    rd = subprocess.run([os.path.join(O.REF_DIR, "deep"), str(nmax)], input=data, capture_output=True, text=True,
+                        check=True, timeout=600)
+    dref = [l for l in rd.stdout.splitlines() if l.startswith("survivor")]
+    assert len(dref) == len(lines)
+    for i, (line, want) in enumerate(zip(lines, dref)):
+        assert f"survivor {i + 1} " + O.deep_line(line, nmax) == want
