@@ -83,3 +83,18 @@ def test_search_feeds_device_recheck(searches):
     outs = ctx().check([E.parse_survivor_line(l) for l in lines], 15, 0)
     verdicts = [E.format_recheck(o, 15) for o in outs]
     assert all(v.startswith("CONSISTENT to n=15") for v in verdicts), verdicts[:3]
+
+
+def test_device_checker_on_survivor_mutants():
+    """The device checker against the oracle on 60 seeded single-cell mutants
+    of real survivors (the oracle equals the reference programs on the same
+    set, tests/test_oracle.py): every recheck and deep verdict kind."""
+    from test_oracle import _mutants
+    lines = _mutants(60, 31)
+    ins = [E.parse_survivor_line(l) for l in lines]
+    outs = ctx().check(ins, 11, 0)
+    for line, o in zip(lines, outs):
+        assert E.format_recheck(o, 11) == O.recheck_line(line, 11)[1], line
+    outs = ctx().check(ins, 11, 1)
+    for ci, o, line in zip(ins, outs, lines):
+        assert E.format_deep(ci, o, 11) == O.deep_line(line, 11), line
