@@ -48,3 +48,13 @@ def test_cli_equals_shipped_output(tmp_path):
     for line, verdicts in pairs:
         want += [line.strip()] + verdicts
     assert p.stdout.splitlines() == want
+
+
+def test_device_equals_oracle_on_survivor_mutants():
+    """check.py on 60 seeded single-cell mutants of real survivors: stage walks
+    that fail early, halts placed in turn into never-read cells, crafted runs
+    that halt, stop or run out."""
+    from test_oracle import _mutants
+    lines = _mutants(60, 31)
+    want = [l for line in lines for l in O.check_line(line)]
+    assert ctx().check_crafted(lines) == want
