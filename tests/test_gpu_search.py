@@ -186,3 +186,39 @@ def test_autotune_keeps_results(searches):
     assert ms > 0 and best.block in (512, 640, 768)
     c, _ = ctx().search(job, best)
     assert c.as_dict()["leaves"] == e["expect"][12]["leaves"]
+
+
+def _budget_symmetry_cases(n, seed):
+    """Jobs that mix an FMAX budget with a symmetry range (the C-ABI allows it;
+    the reference's estimate mode builds such jobs), plus the two symmetry
+    corner cases of setup: no deleted state with LO = 0, and an empty range."""
+    rng = random.Random(seed)
+    base = O.load_machine("erdos_14.txt")
+    out = [("free", -1, ["G0", "H0", "B0"], 0, 0, 9), ("free", 7, ["H0", "H1"], 0, 7, 7)]
+    while len(out) < n:
+        X = rng.randrange(14)
+        lo = rng.randrange(1, 13)
+        hi = rng.randrange(lo, 13)
+        fmax = rng.randint(1, 2)
+        r, job = O.setup(base, X, fmax=fmax, lo=lo, hi=hi)
+        if r >= 0 and job.sym_lo >= 0:
+            out.append(("delete", X, None, fmax, lo, hi))
+    return out
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
+@pytest.mark.parametrize("case", _budget_symmetry_cases(6, 99))
+def test_budget_with_symmetry_vs_oracle(case, kernel):
+    mode, X, free, fmax, lo, hi = case
+    base = O.load_machine("erdos_14.txt")
+    if mode == "free":
+        r, jo = O.setup(base, X, free_cells=free, lo=lo, hi=hi)
+        rd, job = E.setup(base, X, free_cells=free, lo=lo, hi=hi)
+    else:
+        r, jo = O.setup(base, X, fmax=fmax, lo=lo, hi=hi)
+        rd, job = E.setup(base, X, fmax=fmax, lo=lo, hi=hi)
+    assert r >= 0 and rd == 0
+    exp, recs = O.search(jo)
+    c, surv = ctx().search(job, E.tuning(kernel=KERNELS[kernel]))
+    assert c.as_dict() == exp
+    assert sorted(E.survivor_line(job, s) for s in surv) == sorted(O.survivor_line(X, rr, jo.nq) for rr in recs)
