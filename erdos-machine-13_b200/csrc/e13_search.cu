@@ -1080,11 +1080,41 @@ struct CkptClock {
 
 }  // namespace
 
+// Sharding one search (e13_search_shard): the ordering key of a frontier node,
+// every field that identifies the machine and nothing uninitialised.
+struct ShardKey {
+  unsigned short cellv[32];
+  long long t;
+  int p, st, pend, flags, budget, nintro;
+  u64 hb, vmask;
+  bool operator<(const ShardKey &o) const { return memcmp(this, &o, sizeof *this) < 0; }
+};
+
+static ShardKey shard_key(const Node &n) {
+  ShardKey k;
+  memset(&k, 0, sizeof k);
+  memcpy(k.cellv, n.cellv, sizeof k.cellv);
+  k.t = n.t;
+  k.p = n.p;
+  k.st = n.st;
+  k.pend = n.pend;
+  k.flags = n.flags;
+  k.budget = n.budget;
+  k.nintro = n.nintro;
+  k.hb = n.hb;
+  k.vmask = n.vmask;
+  return k;
+}
+
+constexpr long long kSplitPerShard = 512;  // frontier nodes per shard before the deal
+constexpr int kSplitLevels = 24;           // most plain launches of the split
+
 static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning, const e13_checkpoint *ck,
                        e13_counts *counts, e13_survivor *surv, int surv_cap, int *nsurv, double *wall_s,
-                       int64_t *frontier) {
+                       int64_t *frontier, int shard = 0, int nshards = 1) {
   const double t_call = host_seconds();
   if (!c || !job || !counts || !nsurv || (surv_cap > 0 && !surv) || surv_cap < 0) return E13_ERR_ARG;
+  if (nshards < 1 || shard < 0 || shard >= nshards || (ck && nshards > 1)) return E13_ERR_ARG;
   if (job->nq < 1 || job->nq > 16) return E13_ERR_NQ;
   if (job->budget < 0) return E13_ERR_FMAX;
   for (int i = 0; i < 2 * job->nq; ++i)
@@ -1213,6 +1243,63 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
   const int move_blocks = c->nsm * 4;
   long long launches = 0, search_launches = 0;
   int err = 0;
+
+  // sharded: the plain kernel expands the search level by level (each launch
+  // takes the whole frontier) until it holds kSplitPerShard nodes per shard;
+  // the frontier is then put in an order that depends only on its nodes (the
+  // same on every rank) and shard s keeps nodes s, s + nshards, ...  What the
+  // split itself finished (leaves, steps, survivors) counts in shard 0 only.
+  bool split = false;
+  if (nshards > 1) {
+    split = true;
+    Params S = P;
+    CK(cudaFuncSetAttribute(search_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    long long top = 1;
+    for (int level = 0; level < kSplitLevels && top > 0 && top < kSplitPerShard * nshards; ++level) {
+      const long long need = top * (4LL * job->nq + 1) + nwarps * 32 + 1024;
+      if (need > c->out_cap) {
+        CK(cudaStreamSynchronize(c->stream));
+        if ((rc = grow(&c->out, &c->out_cap, need))) return rc;
+      }
+      S.out = c->out;
+      S.out_cap = c->out_cap;
+      search_kernel<false><<<blocks, tu.block, smem, c->stream>>>(S);
+      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, c->stack_cap);
+      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, kWholeFrontier, c->pool_cap);
+      launches += 3;
+      search_launches += 1;
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(c->ctl_host, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (c->ctl_host->error) return E13_ERR_OVERFLOW;
+      top = c->ctl_host->top;
+    }
+    // the deal
+    std::vector<Node> nodes((size_t)top);
+    if (top > 0)
+      CK(cudaMemcpyAsync(nodes.data(), c->stack, sizeof(Node) * (size_t)top, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<std::pair<ShardKey, long long>> order((size_t)top);
+    for (long long i = 0; i < top; ++i) order[(size_t)i] = {shard_key(nodes[(size_t)i]), i};
+    std::sort(order.begin(), order.end(), [](const std::pair<ShardKey, long long> &a,
+                                             const std::pair<ShardKey, long long> &b) { return a.first < b.first; });
+    std::vector<Node> mine;
+    for (long long i = shard; i < top; i += nshards) mine.push_back(nodes[(size_t)order[(size_t)i].second]);
+    if (!mine.empty())
+      CK(cudaMemcpyAsync(c->stack, mine.data(), sizeof(Node) * mine.size(), cudaMemcpyHostToDevice, c->stream));
+    c->ctl_host->top = (long long)mine.size();
+    c->ctl_host->batch = std::min<long long>((long long)mine.size(), batch_max);
+    if (shard != 0) {
+      c->ctl_host->nsurv = 0;
+      CK(cudaMemsetAsync(c->d_jobcnt, 0, sizeof(unsigned long long) * kMaxJobs * kJobCounters, c->stream));
+    }
+    CK(cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    // the split may have grown the output buffer: the main phase uses the new one
+    P.out = c->out;
+    P.out_cap = c->out_cap;
+    P.out_soft = c->out_cap - dump_room - 1024;
+  }
   if (persist) {
     cudaGraph_t graph;
     cudaGraphExec_t exec;
@@ -1295,7 +1382,7 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
   const long long ncopy = std::min<long long>(ns, std::min<long long>(surv_cap, c->surv_cap));
   if (ncopy > 0) {
     std::vector<SurvRec> recs((size_t)ncopy);
-    if (!persist) {
+    if (!persist || split) {
       survivor_read_masks<<<(unsigned)((ncopy + 31) / 32), 32, 0, c->stream>>>(c->surv, ncopy);
       CK(cudaGetLastError());
     }
@@ -1321,6 +1408,11 @@ extern "C" int e13_search_resumable(e13_ctx *c, const e13_job *job, const e13_tu
                                     int *nsurv, double *wall_s, int64_t *frontier) {
   if (!ck || !ck->path || !ck->config || !ck->path[0]) return E13_ERR_ARG;
   return search_impl(c, job, tuning, ck, counts, surv, surv_cap, nsurv, wall_s, frontier);
+}
+
+extern "C" int e13_search_shard(e13_ctx *c, const e13_job *job, const e13_tuning *tuning, int shard, int nshards,
+                                e13_counts *counts, e13_survivor *surv, int surv_cap, int *nsurv) {
+  return search_impl(c, job, tuning, nullptr, counts, surv, surv_cap, nsurv, nullptr, nullptr, shard, nshards);
 }
 
 extern "C" int e13_run_full(e13_ctx *c, const int32_t *tabs, int n, int nq, int64_t *out) {

@@ -142,6 +142,7 @@ def lib():
         L.e13_search_resumable.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Checkpoint), P(Counts),
                                            P(Survivor), I, P(I), P(ctypes.c_double), P(ctypes.c_int64)]
         L.e13_last_stats.argtypes = [ctypes.c_void_p, P(Stats)]
+        L.e13_search_shard.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), I, I, P(Counts), P(Survivor), I, P(I)]
         L.e13_check_crafted.argtypes = [ctypes.c_void_p, P(ctypes.c_char_p), I, ctypes.c_char_p, ctypes.c_size_t,
                                         P(ctypes.c_size_t)]
         L.e13_estimate.argtypes = [ctypes.c_void_p, P(Job), ctypes.c_int64, ctypes.c_uint64, P(EstimateOut),
@@ -172,7 +173,7 @@ def lib():
 
 EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine", "e13_setup",
             "e13_format_survivor", "e13_format_summary", "e13_default_tuning", "e13_ctx_create", "e13_ctx_destroy",
-            "e13_search", "e13_search_resumable", "e13_estimate", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
+            "e13_search", "e13_search_shard", "e13_search_resumable", "e13_estimate", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
             "e13_format_recheck", "e13_format_deep", "e13_check_crafted", "e13_raw_run", "e13_autotune", "e13_check_noalloc",
             "e13_serve_create", "e13_serve_destroy", "e13_serve_clock", "e13_serve_submit", "e13_serve_step",
             "e13_serve_pending", "e13_serve_survivors", "e13_serve_stats"]
@@ -254,6 +255,17 @@ class Context:
                              surv, surv_cap, ctypes.byref(ns))
         if r and r != -7:
             raise E13Error(r, "e13_search")
+        return counts, [surv[i] for i in range(min(ns.value, surv_cap))]
+
+    def search_shard(self, job: Job, shard: int, nshards: int, tune: Tuning | None = None, surv_cap: int = 1 << 16):
+        """Shard `shard` of `nshards` of the search for `job` (e13_search_shard)."""
+        counts = Counts()
+        surv = (Survivor * max(surv_cap, 1))()
+        ns = ctypes.c_int()
+        r = lib().e13_search_shard(self.h, ctypes.byref(job), ctypes.byref(tune) if tune else None, shard, nshards,
+                                   ctypes.byref(counts), surv, surv_cap, ctypes.byref(ns))
+        if r and r != -7:
+            raise E13Error(r, "e13_search_shard")
         return counts, [surv[i] for i in range(min(ns.value, surv_cap))]
 
     def search_resumable(self, job: Job, path: str, config: str, interval_s: float = 0.0,

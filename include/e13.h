@@ -168,6 +168,21 @@ void e13_ctx_destroy(e13_ctx *ctx);
 int e13_search(e13_ctx *ctx, const e13_job *job, const e13_tuning *tuning, e13_counts *counts,
                e13_survivor *surv, int surv_cap, int *nsurv);
 
+/* One share of a search, for spreading one big job over GPUs (one process
+   per GPU).  The reference splits a search over OpenMP threads the same way:
+   a serial expansion to a frontier, whose nodes are then dealt out
+   (src/e13search.c:222-235, 376-403).  Here the plain kernel expands the job
+   level by level until the frontier holds 512 nodes per shard.  The frontier
+   is put in an order that depends only on its nodes, and shard s in [0,
+   nshards) searches nodes s, s + nshards, ...  The leaves, steps and survivors
+   that the expansion itself finishes count in shard 0 only.  So the counts
+   of all shards add up to e13_search's, and their survivors together are its
+   survivors.  Every shard must be given the same job and tuning.  nshards = 1
+   is e13_search.  Returns as e13_search; E13_ERR_ARG for a shard out of
+   range. */
+int e13_search_shard(e13_ctx *ctx, const e13_job *job, const e13_tuning *tuning, int shard, int nshards,
+                     e13_counts *counts, e13_survivor *surv, int surv_cap, int *nsurv);
+
 /* ---- checkpoint / resume of one search ---- */
 
 typedef struct e13_checkpoint {

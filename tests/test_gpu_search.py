@@ -7,7 +7,7 @@ import pytest
 
 import e13b200 as E
 import oracle_lib as O
-from gpu_common import check_entry, ctx, golden_lines, run_entry
+from gpu_common import check_entry, ctx, golden_lines, make_job, run_entry
 
 pytestmark = pytest.mark.gpu
 
@@ -222,3 +222,27 @@ def test_budget_with_symmetry_vs_oracle(case, kernel):
     c, surv = ctx().search(job, E.tuning(kernel=KERNELS[kernel]))
     assert c.as_dict() == exp
     assert sorted(E.survivor_line(job, s) for s in surv) == sorted(O.survivor_line(X, rr, jo.nq) for rr in recs)
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
+@pytest.mark.parametrize("name,X,nshards", [("counter_sym", 13, 4), ("local_edits_f3", 11, 3), ("local_edits_f2", 8, 5)])
+def test_shards_add_up_to_the_search(searches, name, X, nshards, kernel):
+    """e13_search_shard: the shards' counts add up to the golden totals and
+    their survivors together are the golden survivor lines."""
+    entry = searches[name]
+    job = make_job(entry, X)
+    tune = E.tuning(kernel=KERNELS[kernel])
+    tot = None
+    lines = []
+    for s in range(nshards):
+        c, surv = ctx().search_shard(job, s, nshards, tune)
+        d = c.as_dict()
+        tot = d if tot is None else {k: ([a + b for a, b in zip(tot[k], v)] if k == "hist" else tot[k] + v)
+                                     for k, v in d.items()}
+        lines += [E.survivor_line(job, sv) for sv in surv]
+    exp = next(e for e in entry["expect"] if e["X"] == X)
+    assert tot["leaves"] == exp["leaves"] and tot["survivors"] == exp["survivors"] and tot["hist"] == exp["hist"]
+    if exp["steps"] is not None:
+        assert tot["steps"] == exp["steps"]
+    want = [l for l in golden_lines(entry) if l.startswith(f"SURVIVOR X={X} ")]
+    assert sorted(lines) == want

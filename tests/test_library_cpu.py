@@ -217,3 +217,14 @@ def test_setup_random_delete_with_symmetry_matches_oracle():
             assert job.budget == ro
             assert list(job.tab)[: 2 * job.nq] == jo.tab
             assert (job.sym_lo, job.sym_hi, job.sym_n0) == (jo.sym_lo, jo.sym_hi, jo.sym_n0)
+
+
+def test_search_shard_checks_its_arguments():
+    import ctypes
+    base = O.load_machine("erdos_14.txt")
+    r, job = E.setup(base, 11, fmax=2)
+    counts, ns = E.Counts(), ctypes.c_int()
+    L = E.lib()
+    for shard, n in ((0, 0), (2, 2), (-1, 3)):
+        assert L.e13_search_shard(None, ctypes.byref(job), None, shard, n, ctypes.byref(counts), None, 0,
+                                  ctypes.byref(ns)) == -1
