@@ -246,3 +246,27 @@ def test_shards_add_up_to_the_search(searches, name, X, nshards, kernel):
         assert tot["steps"] == exp["steps"]
     want = [l for l in golden_lines(entry) if l.startswith(f"SURVIVOR X={X} ")]
     assert sorted(lines) == want
+
+
+def test_e13gpu_script_prints_the_reference_driver_text(searches):
+    """erdos-machine-13_b200/e13gpu.py, the drop-in for src/e13gpu.py, on the
+    V4 division search: its summary line is the reference driver's
+    (src/e13gpu.py:454-457) with the golden counts."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    entry = searches["division_v4"]
+    exp = entry["expect"][0]
+    args = [os.path.join(root, "tests", "golden", "machines", entry["machine"]), str(exp["X"]), str(entry["lo"]),
+            str(entry["hi"])] + entry["free"]
+    p = subprocess.run([sys.executable, os.path.join(root, "erdos-machine-13_b200", "e13gpu.py")] + args,
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    summary = [l for l in p.stderr.splitlines() if " gpu leaves=" in l]
+    assert len(summary) == 1
+    head = f"X={exp['X']} budget=0 gpu leaves={exp['leaves']} survivors={exp['survivors']} steps={exp['steps']} wall="
+    tail = " dead-at-stage(0..9): " + " ".join(str(h) for h in exp["hist"])
+    assert summary[0].startswith(head) and summary[0].endswith(tail)
+    want = golden_lines(entry) if entry.get("survivors_file") else []
+    assert sorted(l for l in p.stdout.splitlines() if l.strip()) == want

@@ -228,3 +228,25 @@ def test_search_shard_checks_its_arguments():
     for shard, n in ((0, 0), (2, 2), (-1, 3)):
         assert L.e13_search_shard(None, ctypes.byref(job), None, shard, n, ctypes.byref(counts), None, 0,
                                   ctypes.byref(ns)) == -1
+
+
+def _e13gpu(args):
+    import subprocess
+    import sys
+    return subprocess.run([sys.executable, os.path.join(ROOT, "erdos-machine-13_b200", "e13gpu.py")] + args,
+                          capture_output=True, text=True, timeout=120)
+
+
+def test_e13gpu_script_refuses_like_the_reference():
+    """The drop-in for src/e13gpu.py exits 1 with a message on a bad command
+    line, a missing machine file and the symmetry preconditions, before any
+    device work (src/e13gpu.py:79-94, 294-296)."""
+    machine = os.path.join(ROOT, "tests", "golden", "machines", "erdos_14.txt")
+    p = _e13gpu([])
+    assert p.returncode == 1 and "usage" in p.stderr
+    p = _e13gpu(["/nonexistent/m.txt", "9", "-1", "-1", "F0"])
+    assert p.returncode == 1 and "cannot open" in p.stderr
+    p = _e13gpu([machine, "13", "10", "13", "D0"])
+    assert p.returncode == 1 and "named by a fixed cell" in p.stderr
+    p = _e13gpu([machine, "13", "0", "13", "A0", "A1"])
+    assert p.returncode == 1 and ("start state" in p.stderr or "named by a fixed cell" in p.stderr)
