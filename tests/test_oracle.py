@@ -323,3 +323,33 @@ def test_recheck_and_deep_vs_reference_binaries_on_mutants():
     assert len(dref) == len(lines)
     for i, (line, want) in enumerate(zip(lines, dref)):
         assert f"survivor {i + 1} " + O.deep_line(line, nmax) == want
+
+
+@pytest.mark.skipif(not os.path.exists(REFBIN), reason="reference binaries not built here")
+def test_estimate_vs_reference_binary_random():
+    """The restated probe() against the reference binary's estimate mode on one
+    thread, for 6 seeded random jobs (delete with FMAX, free, freesym)."""
+    import random
+    rng = random.Random(404)
+    base = O.load_machine("erdos_14.txt")
+    done = 0
+    while done < 6:
+        X = rng.randrange(14)
+        fmax = rng.randrange(0, 4)
+        cells, lo, hi = [], -1, -1
+        if rng.random() < 0.5:
+            cells = sorted({f"{chr(65 + rng.randrange(14))}{rng.randrange(2)}" for _ in range(rng.randrange(2, 6))})
+            if rng.random() < 0.5:
+                lo = rng.randrange(1, 13)
+                hi = rng.randrange(lo, 13)
+        r, job = O.setup(base, X, fmax=fmax, free_cells=cells or None, lo=lo, hi=hi)
+        if r < 0:
+            continue
+        seed = rng.randrange(1000)
+        args = [REFBIN, "estimate", os.path.join(O.MACHINES, "erdos_14.txt"), "400", str(X), str(fmax), str(lo),
+                str(hi)] + cells
+        p = subprocess.run(args, capture_output=True, text=True, timeout=300,
+                           env=dict(os.environ, OMP_NUM_THREADS="1", E13_SEED=str(seed)))
+        assert p.returncode == 0, p.stderr
+        assert O.estimate_lines(job, 400, seed) == p.stdout.splitlines()[1:5], args
+        done += 1
