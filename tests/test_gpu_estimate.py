@@ -87,3 +87,30 @@ def test_each_kernel_file_has_its_filter_tables(order, tmp_path):
     p = subprocess.run(["python", str(script), os.path.join(ROOT, "erdos-machine-13_b200"),
                         os.path.join(ROOT, "tests")] + list(order), capture_output=True, text=True, timeout=300)
     assert p.returncode == 0 and p.stdout.strip() == "ok", p.stdout + p.stderr
+
+
+def test_device_probes_equal_oracle_on_random_jobs():
+    """Device probes against the oracle on 6 seeded random jobs (delete with
+    FMAX, free, freesym), every probe's four doubles."""
+    import random
+    rng = random.Random(404)
+    base = O.load_machine("erdos_14.txt")
+    done = 0
+    while done < 6:
+        X = rng.randrange(14)
+        fmax = rng.randrange(0, 4)
+        cells, lo, hi = [], -1, -1
+        if rng.random() < 0.5:
+            cells = sorted({f"{chr(65 + rng.randrange(14))}{rng.randrange(2)}" for _ in range(rng.randrange(2, 6))})
+            if rng.random() < 0.5:
+                lo = rng.randrange(1, 13)
+                hi = rng.randrange(lo, 13)
+        ro, ojob = O.setup(base, X, fmax=fmax, free_cells=cells or None, lo=lo, hi=hi)
+        if ro < 0:
+            continue
+        r, job = E.setup(base, X, fmax=fmax, free_cells=cells or None, lo=lo, hi=hi)
+        assert r == 0
+        seed = rng.randrange(1000)
+        out, rows = ctx().estimate(job, 400, seed=seed, per_probe=True)
+        assert rows == O.estimate_per_probe(ojob, 400, seed=seed)
+        done += 1
