@@ -3,19 +3,32 @@
 
 A step is one whole search of the workload: by default the local-edit search
 with FMAX = 4 (delete each of erdos_14's 14 states, <= 4 changed cells; the
-<=4-cell half of the local-edit config, 5,986,617,022 leaves).  The metric is
-simulated Turing-machine steps per second (leaves/s is reported beside it).
+<=4-cell half of the local-edit config, 5,986,617,022 leaves).  Its 14 jobs
+(one per deleted state) run concurrently in one serve session of the
+persistent kernel.  The metric is simulated Turing-machine steps per second,
+with leaves/s beside it.
 
   value     steps of the K timed searches / their device time (CUDA events on
-            the library's stream, summed over the searches of each step)
-  e2e       the same through the public C-ABI call e13_search() timed on the
-            host: root node H2D, control block and survivors D2H included
+            the library's stream, summed over the epochs of each step)
+  e2e       the same search through the public C-ABI serve calls timed on the
+            host clock: job roots host->device, control words, counters and
+            survivor records device->host inside the timed region; the byte
+            counts are the library's own (e13_stats h2d_bytes / d2h_bytes)
   roofline  integer-issue bound of the search kernel: 16 lane-ops per step
             against SMs x 128 lanes x the SM clock sampled during the run
   cpu_baseline  the reference's own e13search (OpenMP, all host threads) on a
-            bounded sample: the FMAX = 3 local-edit search
+            bounded sample, the FMAX = 3 local-edit search; same_sample gives
+            the GPU's rate on that same search beside it
+  kernels   the persistent kernel against the plain per-frontier kernel on
+            the FMAX = 4 search and on the counter search, each job run alone
+            one after another on both kernels (like for like)
+  serving   the serving mix: a seeded Poisson stream of 40 jobs (p50/p99)
+  raw_set   the raw-simulator set: 1e6 random 13-state machines, <= 2^18 steps
 
---impl reference runs that reference CPU program instead (the reference arm).
+Every measured search is checked against the reference's logs (leaves,
+survivors, deaths per stage, steps where logged, sorted survivor lines).
+
+--impl reference runs the reference CPU program instead (the reference arm).
 Under torchrun (N > 1) rank r runs every N-th X starting at r (the search
 splits into independent per-X jobs; e13shard.py sums the totals and takes the
 maximum of the times over ranks).
@@ -23,8 +36,10 @@ maximum of the times over ranks).
 from __future__ import annotations
 
 import argparse
+import gzip
 import json
 import os
+import random
 import statistics
 import subprocess
 import sys
@@ -33,93 +48,158 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "erdos-machine-13_b200"))
-sys.path.insert(0, os.path.join(ROOT, "tests"))
-MACHINES = os.path.join(ROOT, "tests", "golden", "machines")
+GOLD = os.path.join(ROOT, "tests", "golden")
+MACHINES = os.path.join(GOLD, "machines")
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "e13search")
 
 WORKLOADS = {
     "local_edits_f4": dict(desc="delete erdos_14 FMAX=4 X=0..13", machine="erdos_14.txt", mode="delete", fmax=4,
-                           X=list(range(14)), leaves=5986617022),
+                           X=list(range(14)), golden="local_edits_f4"),
     "local_edits_f3": dict(desc="delete erdos_14 FMAX=3 X=0..13", machine="erdos_14.txt", mode="delete", fmax=3,
-                           X=list(range(14)), leaves=36383467),
+                           X=list(range(14)), golden="local_edits_f3"),
+    "local_edits_f2": dict(desc="delete erdos_14 FMAX=2 X=0..13", machine="erdos_14.txt", mode="delete", fmax=2,
+                           X=list(range(14)), golden="local_edits_f2"),
     "counter_sym": dict(desc="freesym erdos_14 13 10 13 D0 G0 K0 K1 L1 M1", machine="erdos_14.txt", mode="freesym",
-                        X=[13], free=["D0", "G0", "K0", "K1", "L1", "M1"], lo=10, hi=13, leaves=3078656272),
+                        X=[13], free=["D0", "G0", "K0", "K1", "L1", "M1"], lo=10, hi=13, golden="counter_sym"),
     "division_v4": dict(desc="freesym erdos_14 9 3 9 F0..I1", machine="erdos_14.txt", mode="freesym", X=[9],
-                        free=["F0", "F1", "G0", "G1", "H0", "H1", "I0", "I1"], lo=3, hi=9, leaves=830955779),
+                        free=["F0", "F1", "G0", "G1", "H0", "H1", "I0", "I1"], lo=3, hi=9, golden="division_v4"),
+    "serving_mix": dict(desc="seeded Poisson stream of 40 search jobs on erdos_14 (seed 2026, 25 jobs/s): random "
+                             "deleted state, random free set of 2-8 cells (symmetry where setup allows) or FMAX "
+                             "2-4, plus counter_sym and FMAX=4 X=11", machine="erdos_14.txt", mode="mix", X=[]),
 }
-WORKLOADS["serving_mix"] = dict(desc="seeded Poisson stream of 40 search jobs on erdos_14 (seed 2026, 25 jobs/s): "
-                                    "random deleted state, random free set of 2-5 cells (symmetry where setup "
-                                    "allows) or FMAX 2-4, plus counter_sym and FMAX=4 X=11",
-                               machine="erdos_14.txt", mode="mix", X=[], leaves=None)
 CPU_SAMPLE = "local_edits_f3"
+OPS_PER_STEP = 16  # integer lane-ops per simulated step (hash test 2, deadline 1, address 1, load+extract 2,
+#                    index 1, table 2, fork test 1, halt test 1, write test 1, head 2, bounds 2)
+NODE_BYTES = 320   # one frontier node (e13dev::Node)
 
 
-def serving_mix(seed=2026, n=40, rate=25.0):
-    """The serving-mix job stream: (kind, X, cells, fmax, lo, hi) and arrival times."""
-    import random
+def golden(name):
+    with open(os.path.join(GOLD, "searches.json")) as f:
+        return next(e for e in json.load(f) if e["name"] == name)
 
-    import oracle_lib as O
 
+def golden_lines(entry):
+    if not entry.get("survivors_file"):
+        return []
+    fn = os.path.join(GOLD, entry["survivors_file"])
+    op = gzip.open if fn.endswith(".gz") else open
+    with op(fn, "rt") as f:
+        return sorted(l.rstrip("\n") for l in f if l.strip())
+
+
+def parity_of(w, per_job, lines):
+    """Each job's counts against the reference's log for its X, and the sorted
+    survivor lines against the reference's survivor file."""
+    g = golden(w["golden"])
+    exp = {e["X"]: e for e in g["expect"]}
+    ok = {"leaves": True, "survivors": True, "hist": True, "steps": True}
+    steps_checked = 0
+    for X, c in per_job.items():
+        e = exp[X]
+        ok["leaves"] &= c.leaves == e["leaves"]
+        ok["survivors"] &= c.survivors == e["survivors"]
+        ok["hist"] &= list(c.hist) == e["hist"]
+        if e["steps"] is not None:
+            ok["steps"] &= c.steps == e["steps"]
+            steps_checked += 1
+    ok["survivor_lines"] = sorted(lines) == golden_lines(g) if g.get("survivors_file") else (len(lines) == 0)
+    ok["jobs_with_logged_steps"] = steps_checked
+    ok["all"] = all(v for k, v in ok.items() if k != "jobs_with_logged_steps")
+    return ok
+
+
+def parse_summary(line):
+    """Fields of a reference summary line (src/e13search.c:413-416)."""
+    out = {}
+    for tok in line.split():
+        if "=" in tok:
+            k, v = tok.split("=", 1)
+            if k in ("leaves", "survivors", "steps"):
+                out[k] = int(v)
+    return out
+
+
+def make_jobs(E, w, xs=None):
+    base = E.load_machine(os.path.join(MACHINES, w["machine"]))
+    jobs = []
+    for X in (w["X"] if xs is None else xs):
+        if w["mode"] == "delete":
+            r, job = E.setup(base, X, fmax=w["fmax"])
+        else:
+            r, job = E.setup(base, X, free_cells=w["free"], lo=w.get("lo", -1), hi=w.get("hi", -1))
+        if r == 0:
+            jobs.append((X, job))
+    return jobs
+
+
+MIX_MAX_LEAVES = 1e10  # the stream's job sizes span 1e3 .. 1e10 leaves
+
+
+def serving_mix(E, ctx, seed=2026, n=40, rate=25.0):
+    """The serving-mix job stream: a list of (Job, arrival time).  Jobs are set
+    up with the library's own e13_setup; one whose setup the reference would
+    refuse is redrawn, symmetry falls back to off where setup rejects it, and a
+    free-set job whose size estimate (e13_estimate, 256 probes, seed 0: the
+    same doubles on every run) exceeds 1e10 leaves is redrawn."""
     rng = random.Random(seed)
-    base = O.load_machine("erdos_14.txt")
+    base = E.load_machine(os.path.join(MACHINES, "erdos_14.txt"))
     cells_all = [f"{chr(65 + q)}{a}" for q in range(14) for a in (0, 1)]
     out, t = [], 0.0
     while len(out) < n:
         t += rng.expovariate(rate)
         X = rng.randrange(14)
         if len(out) == n // 3:
-            out.append((("free", 13, ["D0", "G0", "K0", "K1", "L1", "M1"], 0, 10, 13), t))  # counter_sym
+            r, job = E.setup(base, 13, free_cells=["D0", "G0", "K0", "K1", "L1", "M1"], lo=10, hi=13)
+            out.append((job, t))  # counter_sym, 3.1e9 leaves
             continue
         if len(out) == 2 * n // 3:
-            out.append((("delete", 11, None, 4, -1, -1), t))
+            r, job = E.setup(base, 11, fmax=4)
+            out.append((job, t))  # the largest FMAX = 4 job
             continue
         if rng.random() < 0.5:
-            cells = rng.sample([c for c in cells_all if ord(c[0]) - 65 != X], rng.randint(2, 5))
+            k = rng.randint(2, 8)
+            cells = rng.sample([c for c in cells_all if ord(c[0]) - 65 != X], k)
             lo = hi = -1
             if rng.random() < 0.5:
                 lo, hi = sorted(rng.sample(range(1, 14), 2))
-                if not (lo <= X <= hi) or O.setup(base, X, free_cells=cells, lo=lo, hi=hi)[0] < 0:
+                if not (lo <= X <= hi) or E.setup(base, X, free_cells=cells, lo=lo, hi=hi)[0] != 0:
                     lo = hi = -1  # symmetry only where setup() accepts it
-            if O.setup(base, X, free_cells=cells, lo=lo, hi=hi)[0] < 0:
+            r, job = E.setup(base, X, free_cells=cells, lo=lo, hi=hi)
+            if r != 0:
                 continue
-            out.append((("free", X, cells, 0, lo, hi), t))
+            est, _ = ctx.estimate(job, 256, 0)
+            if est.mean[0] > MIX_MAX_LEAVES:
+                continue  # 7-8 free cells without symmetry reach 1e11+ leaves
+            out.append((job, t))
         else:
             fmax = rng.randint(2, 4)
             if fmax == 4 and rng.random() < 0.7:
-                fmax = 3  # keep most jobs small: the stream spans 1e3 .. 1e9 leaves
-            if O.setup(base, X, fmax=fmax)[0] < 0:
+                fmax = 3  # keep most jobs small
+            r, job = E.setup(base, X, fmax=fmax)
+            if r != 0:
                 continue
-            out.append((("delete", X, None, fmax, -1, -1), t))
+            out.append((job, t))
     return out
-# DRAM bytes (read + write) of one 200 ms epoch launch of the persistent search
-# kernel, from the ncu capture summarised in
-# profiles/search_kernel_persistent_local_edits_f4.md
-PROFILED_TRAFFIC = {"local_edits_f4": 386.7e6}
-OPS_PER_STEP = 16  # integer lane-ops per simulated step (hash test 2, deadline 1, address 1, load+extract 2,
-#                    index 1, table 2, fork test 1, halt test 1, write test 1, head 2, bounds 2)
-
-
-def ref_args(w):
-    path = os.path.join(MACHINES, w["machine"])
-    if w["mode"] == "delete":
-        return ["delete", path, str(w["fmax"])] + [str(x) for x in w["X"]]
-    if w["mode"] == "freesym":
-        return ["freesym", path, str(w["X"][0]), str(w["lo"]), str(w["hi"])] + w["free"]
-    return ["free", path, str(w["X"][0])] + w["free"]
 
 
 def run_reference_cpu(w, threads):
     """The reference's e13search on the host cores; returns (steps, leaves, seconds, kind)."""
-    import oracle_lib as O
-
     if os.path.exists(REF_BIN):
+        path = os.path.join(MACHINES, w["machine"])
+        if w["mode"] == "delete":
+            args = ["delete", path, str(w["fmax"])] + [str(x) for x in w["X"]]
+        else:
+            args = ["freesym", path, str(w["X"][0]), str(w["lo"]), str(w["hi"])] + w["free"]
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         t0 = time.perf_counter()
-        r = subprocess.run([REF_BIN] + ref_args(w), capture_output=True, text=True, env=env, check=True)
+        r = subprocess.run([REF_BIN] + args, capture_output=True, text=True, env=env, check=True)
         dt = time.perf_counter() - t0
-        s = [O.parse_summary(l) for l in r.stderr.splitlines() if "leaves=" in l]
+        s = [parse_summary(l) for l in r.stderr.splitlines() if "leaves=" in l]
         return sum(x["steps"] for x in s), sum(x["leaves"] for x in s), dt, "reference"
     # no reference build on this machine: the oracle's restatement (same algorithm, pthreads)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+
     base = O.load_machine(w["machine"])
     steps = leaves = 0
     t0 = time.perf_counter()
@@ -203,7 +283,7 @@ def reference_arm(args, w, ws, rank, pg):
     threads = os.cpu_count() or 1
     sample = WORKLOADS[CPU_SAMPLE]
     for _ in range(args.warmup):
-        run_reference_cpu(sample, threads)
+        run_reference_cpu(WORKLOADS["local_edits_f2"], threads)  # pages the program and its data in
     tot_steps = tot_leaves = 0
     tot_t = 0.0
     kind = "reference"
@@ -220,62 +300,129 @@ def reference_arm(args, w, ws, rank, pg):
             "config": {"workload": f"{CPU_SAMPLE}: {sample['desc']} (bounded sample of {w['desc']})",
                        "sample_of": args.workload},
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": kind,
-                             "sample": f"{sample['desc']} per step"},
+                             "sample": f"{sample['desc']} per step (4.0e9 steps)"},
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()
 
 
-def serving_bench(args, w, ws, rank, local, pg):
-    """The serving workload: search jobs arrive as a Poisson stream and join the
-    running persistent kernel as job slots and frontier memory free up."""
-    import torch
+def roofline(steps, seconds, sm_mhz, nsm):
+    peak = nsm * 128 * sm_mhz * 1e6 / 1e9
+    ach = OPS_PER_STEP * steps / seconds / 1e9
+    return {"bound": "int-issue", "achieved": ach, "peak": peak, "unit": "Gop/s", "frac": ach / peak}
 
-    import e13b200 as E
-    import oracle_lib as O
 
-    base = O.load_machine("erdos_14.txt")
-    stream = serving_mix()
-    jobs, arrivals = [], []
-    for (kind, X, cells, fmax, lo, hi), t in stream:
-        if kind == "free":
-            r, job = E.setup(base, X, free_cells=cells, lo=lo, hi=hi)
-        else:
-            r, job = E.setup(base, X, fmax=fmax)
-        assert r == 0
-        jobs.append(job)
-        arrivals.append(t)
-    ctx = E.Context(local)
-    lat, steps, dev_ms, wall, leaves, epochs, launches = [], 0, 0.0, 0.0, [], 0, 0
-    for it in range(args.warmup + args.steps):
+def run_concurrent(E, ctx, jobs, epoch_us=200000, stack_nodes=0):
+    """All jobs in one serve session of the persistent kernel.  Returns
+    ({X: Counts}, survivor lines, device ms, launches, h2d, d2h, wall s)."""
+    per, lines = {}, []
+    t0 = time.perf_counter()
+    with E.Server(ctx, E.tuning(epoch_us=epoch_us, stack_nodes=stack_nodes)) as srv:
+        got = srv.run_all([j for _, j in jobs])
+        ms, _ = srv.stats()
+    wall = time.perf_counter() - t0
+    st = ctx.stats()
+    for i, (X, job) in enumerate(jobs):
+        r, surv = got[i]
+        per[X] = r.counts
+        lines += [E.survivor_line(job, s) for s in surv]
+    return per, lines, ms, st.launches, st.h2d_bytes, st.d2h_bytes, wall
+
+
+def run_sequential(E, ctx, jobs, kernel):
+    """Each job alone with e13_search on one kernel, one after another."""
+    per, lines, ms, launches = {}, [], 0.0, 0
+    for X, job in jobs:
+        c, surv = ctx.search(job, E.tuning(kernel=kernel))
+        st = ctx.stats()
+        per[X] = c
+        lines += [E.survivor_line(job, s) for s in surv]
+        ms += st.device_ms
+        launches += st.launches
+    return per, lines, ms, launches
+
+
+def kernel_comparison(E, torch, ctx, flush, local, nsm):
+    """Persistent vs plain on the same searches, both run the same way: each
+    job of the workload alone, one after another."""
+    out = {}
+    for name in ("local_edits_f4", "counter_sym"):
+        w = WORKLOADS[name]
+        jobs = make_jobs(E, w)
+        entry = {"workload": w["desc"], "jobs": f"{len(jobs)} job(s), each alone, one after another"}
+        for kname, k in (("persistent", E.KERNEL_PERSISTENT), ("plain", E.KERNEL_PLAIN)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            sampler = ClockSampler(local)
+            with sampler:
+                per, lines, ms, launches = run_sequential(E, ctx, jobs, k)
+            clocks = sampler.summary()
+            steps = sum(c.steps for c in per.values())
+            leaves = sum(c.leaves for c in per.values())
+            entry[kname] = {"steps_per_s": steps / (ms / 1000), "leaves_per_s": leaves / (ms / 1000),
+                            "device_ms": ms, "gpu_launches": launches,
+                            "roofline": roofline(steps, ms / 1000, clocks["sm_mhz"] or 1965.0, nsm),
+                            "clocks": clocks, "parity": parity_of(w, per, lines)}
+        entry["persistent_over_plain"] = entry["persistent"]["steps_per_s"] / entry["plain"]["steps_per_s"]
+        out[name] = entry
+    return out
+
+
+def serving_stats(E, ctx, stream, reps=1):
+    lat, steps, dev_ms, wall, leaves, launches = [], 0, 0.0, 0.0, [], 0
+    status_ok = True
+    for _ in range(reps):
         with E.Server(ctx) as srv:
             t0 = time.perf_counter()
-            got = srv.run_all(jobs, arrivals)
+            got = srv.run_all([j for j, _ in stream], [t for _, t in stream])
             dt = time.perf_counter() - t0
-            ms, ep = srv.stats()
-        if it >= args.warmup:
-            wall += dt
-            dev_ms += ms
-            epochs += ep
-            launches += ctx.stats().launches
-            for r, surv in got.values():
-                steps += r.counts.steps
-                lat.append(r.t_done - r.t_submit)
-                leaves.append(r.counts.leaves)
+            ms, _ = srv.stats()
+        wall += dt
+        dev_ms += ms
+        launches += ctx.stats().launches
+        for r, _ in got.values():
+            status_ok &= r.status == 0
+            steps += r.counts.steps
+            lat.append(r.t_done - r.t_submit)
+            leaves.append(r.counts.leaves)
     lat.sort()
     p = lambda q: lat[min(len(lat) - 1, int(q * len(lat)))]
-    line = {"metric": "TM steps/s", "value": steps / wall, "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000 * wall / args.steps, "higher_is_better": True,
+    return {"steps_per_s": steps / wall, "wall_s": wall / reps, "jobs": len(stream), "leaves_min": min(leaves),
+            "leaves_max": max(leaves), "latency_p50_s": p(0.50), "latency_p90_s": p(0.90), "latency_p99_s": p(0.99),
+            "device_busy_frac": dev_ms / 1000 / wall, "gpu_launches": launches, "all_jobs_ok": status_ok,
+            "note": "steps of all jobs / wall time from the first arrival to the last completion; jobs arrive on "
+                    "the host clock, so idle gaps between arrivals count"}
+
+
+def serving_bench(args, w, ws, rank, local, pg):
+    """The serving workload as the headline: search jobs arrive as a Poisson
+    stream and join the running persistent kernel as slots and memory free up."""
+    import e13b200 as E
+
+    ctx = E.Context(local)
+    stream = serving_mix(E, ctx)
+    for _ in range(args.warmup):
+        serving_stats(E, ctx, stream)
+    s = serving_stats(E, ctx, stream, reps=args.steps)
+    line = {"metric": "TM steps/s", "value": s["steps_per_s"], "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * s["wall_s"], "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "int32+u64", "data": "synthetic (seeded job stream)",
-            "config": {"workload": f"serving_mix: {w['desc']}", "kernel": "persistent (serve)",
-                       "jobs": len(jobs), "leaves_min": min(leaves), "leaves_max": max(leaves)},
-            "latency_p50_s": p(0.50), "latency_p99_s": p(0.99),
-            "device_busy_frac": dev_ms / 1000 / wall, "gpu_launches": launches,
-            "note": "value = steps of all jobs / wall time from the first arrival to the last completion; "
-                    "jobs arrive on the host clock, so idle gaps between arrivals count"}
+            "config": {"workload": f"serving_mix: {w['desc']}", "kernel": "persistent (serve)"}, "serving": s,
+            "gpu_launches": s["gpu_launches"]}
     print(json.dumps(line), flush=True)
     ctx.close()
+
+
+def raw_set(E, ctx):
+    n = 1_000_000
+    _, tot = ctx.raw_run(n, seed=0, want_out=False)
+    ms = ctx.stats().device_ms
+    with open(os.path.join(GOLD, "raw_1e6.json")) as f:
+        g = json.load(f)
+    return {"machines": n, "total_steps": tot, "device_ms": ms, "steps_per_s": tot / (ms / 1000),
+            "parity_total_steps": tot == g["total_steps"],
+            "note": "1e6 random 13-state tables from seed 0, <= 2^18 steps, no filter; tables drawn on the device"}
 
 
 def main():
@@ -285,8 +432,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="local_edits_f4", choices=list(WORKLOADS))
-    ap.add_argument("--kernel", default="persistent", choices=["persistent", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="headline only (no kernel comparison, serving, raw set)")
+    ap.add_argument("--stack-nodes", type=int, default=0, help="frontier capacity of the serve session (0: default)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     ws, rank, local, pg = dist_setup()
@@ -296,64 +444,22 @@ def main():
     import torch
 
     import e13b200 as E
-    import oracle_lib as O
 
     torch.cuda.set_device(local)
     if args.workload == "serving_mix":
         return serving_bench(args, w, ws, rank, local, pg)
     import e13shard as S
 
-    base = O.load_machine(w["machine"])
-    jobs = []
-    for X in S.share(w["X"], rank, ws):
-        if w["mode"] == "delete":
-            r, job = E.setup(base, X, fmax=w["fmax"])
-        else:
-            r, job = E.setup(base, X, free_cells=w["free"], lo=w.get("lo", -1), hi=w.get("hi", -1))
-        if r == 0:
-            jobs.append(job)
-    kernel = E.KERNEL_PERSISTENT if args.kernel == "persistent" else E.KERNEL_PLAIN
-    tune = E.tuning(kernel=kernel)
+    jobs = make_jobs(E, w, S.share(w["X"], rank, ws))
     ctx = E.Context(local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
-
-    kstats = dict(epochs=0, jobs=len(jobs))
-
-    def one_step():
-        """One whole search of the workload.  Persistent kernel: all of its jobs
-        (one per deleted state X) run concurrently in one serve session.  Plain
-        kernel: the jobs run one after another, one launch per frontier batch."""
-        steps = leaves = 0
-        dev_ms = 0.0
-        launches = 0
-        surv_bytes = 0
-        if kernel == E.KERNEL_PERSISTENT:
-            with E.Server(ctx, E.tuning(epoch_us=200000)) as srv:
-                got = srv.run_all(jobs)
-                ms, epochs = srv.stats()
-            for r, surv in got.values():
-                steps += r.counts.steps
-                leaves += r.counts.leaves
-                surv_bytes += 64 * len(surv)
-            dev_ms = ms
-            launches = ctx.stats().launches  # search, move, finish, node count per epoch; frontier order
-            kstats["epochs"] += epochs
-        else:
-            for job in jobs:
-                c, surv = ctx.search(job, tune)
-                st = ctx.stats()
-                steps += c.steps
-                leaves += c.leaves
-                dev_ms += st.device_ms
-                launches += st.launches
-                surv_bytes += 64 * len(surv)
-                kstats["epochs"] += st.epochs
-        return steps, leaves, dev_ms, launches, surv_bytes
+    nsm = torch.cuda.get_device_properties(local).multi_processor_count
 
     for _ in range(args.warmup):
-        one_step()
+        run_concurrent(E, ctx, jobs, stack_nodes=args.stack_nodes)
     torch.cuda.synchronize()
-    tot = dict(steps=0, leaves=0, dev_ms=0.0, wall=0.0, launches=0, d2h=0)
+    tot = dict(steps=0, leaves=0, dev_ms=0.0, wall=0.0, launches=0, h2d=0, d2h=0)
+    per_all, lines_all = {}, []
     sampler = ClockSampler(local)
     if pg:
         pg.barrier()
@@ -361,54 +467,64 @@ def main():
         for _ in range(args.steps):
             flush.zero_()  # evict L2 (126 MB) between timed steps
             torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            s, l, ms, nl, d2h = one_step()
+            per, lines, ms, nl, h2d, d2h, wall = run_concurrent(E, ctx, jobs, stack_nodes=args.stack_nodes)
             torch.cuda.synchronize()
-            tot["wall"] += time.perf_counter() - t0
-            tot["steps"] += s
-            tot["leaves"] += l
+            tot["wall"] += wall
+            tot["steps"] += sum(c.steps for c in per.values())
+            tot["leaves"] += sum(c.leaves for c in per.values())
             tot["dev_ms"] += ms
             tot["launches"] += nl
+            tot["h2d"] += h2d
             tot["d2h"] += d2h
+            per_all, lines_all = per, lines
     if pg:
         pg.barrier()
     clocks = sampler.summary()
+    par = parity_of(w, per_all, lines_all) if ws == 1 else None
     if pg:
-        sums, maxes = S.reduce_totals(pg, {k: tot[k] for k in ("steps", "leaves", "launches", "d2h")},
+        sums, maxes = S.reduce_totals(pg, {k: tot[k] for k in ("steps", "leaves", "launches", "h2d", "d2h")},
                                       {k: tot[k] for k in ("dev_ms", "wall")}, device=f"cuda:{local}")
         tot.update(sums)
         tot.update(maxes)
-    parity = tot["leaves"] == w["leaves"] * args.steps
     dev_s = tot["dev_ms"] / 1000.0
     value = tot["steps"] / dev_s
     sm_mhz = clocks["sm_mhz"] or 1965.0
-    nsm = torch.cuda.get_device_properties(local).multi_processor_count
-    peak_gops = nsm * 128 * sm_mhz * 1e6 / 1e9
-    ach_gops = OPS_PER_STEP * tot["steps"] / dev_s / 1e9
+    rl = roofline(tot["steps"], dev_s, sm_mhz, nsm)
+    rl.update({"traffic": None, "note": f"{OPS_PER_STEP} integer lane-ops per step; peak = {nsm} SMs x 128 lanes x "
+                                        f"{sm_mhz:.0f} MHz (median SM clock sampled during the timed region); "
+                                        "DRAM traffic is not the bound (see the profile summary)"})
     line = {"metric": "TM steps/s", "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot["dev_ms"] / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "int32+u64", "data": "synthetic (reference searches)",
-            "leaves_per_s": tot["leaves"] / dev_s, "parity": parity,
-            "config": {"workload": f"{args.workload}: {w['desc']}", "kernel": args.kernel,
-                       "jobs": "concurrent in one persistent kernel" if kernel == E.KERNEL_PERSISTENT
-                       else "one after another",
-                       "leaves_per_step": w["leaves"], "l2": "flushed between steps (256 MiB write)",
+            "leaves_per_s": tot["leaves"] / dev_s, "parity": par,
+            "config": {"workload": f"{args.workload}: {w['desc']}", "kernel": "persistent",
+                       "jobs": f"{len(jobs)} job(s) concurrent in one serve session",
+                       "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"X sharded over {ws} rank(s)"},
-            "roofline": {"bound": "int-issue", "achieved": ach_gops, "peak": peak_gops, "unit": "Gop/s",
-                         "frac": ach_gops / peak_gops, "traffic": PROFILED_TRAFFIC.get(args.workload),
-                         "note": f"{OPS_PER_STEP} integer lane-ops per step; peak = {nsm} SMs x 128 lanes x "
-                                 f"{sm_mhz:.0f} MHz (median SM clock sampled during the timed region)"},
+            "roofline": rl,
             "e2e": {"value": tot["steps"] / tot["wall"], "unit": "steps/s",
-                    "h2d_bytes_per_step": 288 * len(jobs) + 160 * len(jobs),
-                    "d2h_bytes_per_step": tot["d2h"] // args.steps + 160 * len(jobs)},
-            "gpu_launches": tot["launches"], "clocks": clocks,
-            "kernel_stats": {"epochs": kstats["epochs"], "jobs_per_step": kstats["jobs"],
-                             "note": "epochs over all warmup and timed steps"}}
+                    "h2d_bytes_per_step": tot["h2d"] // args.steps, "d2h_bytes_per_step": tot["d2h"] // args.steps,
+                    "note": "host clock around the C-ABI serve calls (create, submit, step until done, destroy)"},
+            "gpu_launches": tot["launches"], "clocks": clocks}
+    if rank == 0 and ws == 1 and not args.no_extras:
+        line["kernels"] = kernel_comparison(E, torch, ctx, flush, local, nsm)
+        stream = serving_mix(E, ctx)
+        serving_stats(E, ctx, stream)  # warm-up of the stream's job shapes
+        line["serving"] = serving_stats(E, ctx, stream)
+        line["raw_set"] = raw_set(E, ctx)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        s, l, dt, kind = run_reference_cpu(WORKLOADS[CPU_SAMPLE], threads)
+        sw = WORKLOADS[CPU_SAMPLE]
+        s, l, dt, kind = run_reference_cpu(sw, threads)
         line["cpu_baseline"] = {"value": s / dt, "unit": "steps/s", "cores": threads, "kind": kind,
-                                "sample": WORKLOADS[CPU_SAMPLE]["desc"] + " (4.0e9 steps)"}
+                                "sample": sw["desc"] + " (4.0e9 steps)"}
+        flush.zero_()
+        torch.cuda.synchronize()
+        per, lines, ms, *_ = run_concurrent(E, ctx, make_jobs(E, sw))
+        gsteps = sum(c.steps for c in per.values())
+        line["same_sample"] = {"workload": sw["desc"], "gpu_steps_per_s": gsteps / (ms / 1000),
+                               "cpu_steps_per_s": s / dt, "gpu_over_cpu": (gsteps / (ms / 1000)) / (s / dt),
+                               "parity": parity_of(sw, per, lines)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

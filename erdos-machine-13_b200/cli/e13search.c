@@ -9,7 +9,10 @@
      e13search estimate machine.txt PROBES X FMAX LO HI [CELL...]
 
    Survivors go to stdout in the reference's format, one summary line per X to
-   stderr.  Environment: E13_DEVICE (CUDA device, default 0), E13_KERNEL
+   stderr.  estimate prints the reference's four lines; its probes are drawn
+   from per-probe streams (at most 2^20 probes), so the numbers are another
+   sample of the same estimator: they equal the reference probe for probe, not
+   line for line.  Environment: E13_DEVICE (CUDA device, default 0), E13_KERNEL
    (persistent | plain).  There is no CPU path: without a GPU it exits 1.
 
    free / freesym keep checkpoints as src/e13gpu.py:349-409 does: E13_CKPT
@@ -90,7 +93,10 @@ static int run_one(e13_ctx *ctx, const e13_job *job, const e13_tuning *tu, const
 
 int main(int argc, char **argv) {
   if (argc < 3) {
-    fprintf(stderr, "usage: e13search base|mutant|delete|free|freesym machine.txt [FMAX X...]\n");
+    fprintf(stderr,
+            "usage: e13search base|mutant|delete|free|freesym machine.txt [FMAX X...]\n"
+            "       e13search estimate machine.txt PROBES X FMAX LO HI [CELL...]   (PROBES <= 1048576; a\n"
+            "       different sample than the reference's: equal probe for probe, not line for line)\n");
     return 1;
   }
   int32_t base[E13_MAXCELLS];

@@ -16,6 +16,8 @@
 // word under the head stays in a register; runs of a self-loop are crossed a
 // word at a time.
 #include <cuda_runtime.h>
+
+#include <mutex>
 #include <stdio.h>
 #include <string.h>
 
@@ -346,26 +348,34 @@ static __device__ __align__(256) e13_check_in g_noalloc_in[E13_CHECK_NOALLOC_MAX
 static __device__ __align__(256) e13_check_out g_noalloc_out[E13_CHECK_NOALLOC_MAX];
 
 constexpr int kNoAllocMaxDevices = 64;
-struct NoAllocAddrs {
-  bool ready;
+// Per device, filled once under std::call_once: the arrays' device addresses
+// and a non-blocking stream of this entry point's own, so a call waits for its
+// own work only (not for other streams of the device, and not for a capture
+// another thread holds on the legacy default stream).
+struct NoAllocDevice {
+  std::once_flag once;
+  int rc;
   u32 *tapes;
   e13_check_in *in;
   e13_check_out *out;
+  cudaStream_t stream;
 };
-NoAllocAddrs g_noalloc_addrs[kNoAllocMaxDevices];
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
 
-int noalloc_addresses(int device, NoAllocAddrs **out) {
+// With `device` current.
+int noalloc_device(int device, NoAllocDevice **out) {
   if (device < 0 || device >= kNoAllocMaxDevices) return E13_ERR_ARG;
-  NoAllocAddrs &a = g_noalloc_addrs[device];
-  if (!a.ready) {
-    if (cudaGetSymbolAddress((void **)&a.tapes, g_noalloc_tapes) != cudaSuccess ||
-        cudaGetSymbolAddress((void **)&a.in, g_noalloc_in) != cudaSuccess ||
-        cudaGetSymbolAddress((void **)&a.out, g_noalloc_out) != cudaSuccess)
-      return E13_ERR_CUDA;
-    a.ready = true;
-  }
-  *out = &a;
-  return E13_OK;
+  NoAllocDevice &d = g_noalloc_dev[device];
+  std::call_once(d.once, [&d]() {
+    d.rc = E13_OK;
+    if (cudaGetSymbolAddress((void **)&d.tapes, g_noalloc_tapes) != cudaSuccess ||
+        cudaGetSymbolAddress((void **)&d.in, g_noalloc_in) != cudaSuccess ||
+        cudaGetSymbolAddress((void **)&d.out, g_noalloc_out) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking) != cudaSuccess)
+      d.rc = E13_ERR_CUDA;
+  });
+  *out = &d;
+  return d.rc;
 }
 
 }  // namespace
@@ -377,9 +387,10 @@ extern "C" int e13_check_noalloc(int device, const e13_check_in *in, int n, int 
   if (n > E13_CHECK_NOALLOC_MAX) return E13_ERR_NOALLOC_SIZE;
   if (n == 0) return E13_OK;
   if (cudaSetDevice(device) != cudaSuccess) return E13_ERR_CUDA;
-  NoAllocAddrs *a = nullptr;
-  int rc = noalloc_addresses(device, &a);
+  NoAllocDevice *a = nullptr;
+  int rc = noalloc_device(device, &a);
   if (rc) return rc;
+  const cudaStream_t st = a->stream;
   const bool deep = mode == E13_CHECK_DEEP;
   const int W = (int)((kWinLeft + (1LL << nmax) + 4096 + 31) / 32 + 2);
   const int nl = (int)std::min<i64>(32, kSmemBudget / ((i64)W * 4));
@@ -388,9 +399,9 @@ extern "C" int e13_check_noalloc(int device, const e13_check_in *in, int n, int 
   if (cudaFuncSetAttribute(check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return E13_ERR_CUDA;
   // the arrays keep the previous call's contents: clear the tapes and outputs
-  if ((!deep && cudaMemset(a->tapes, 0, sizeof(u32) * (size_t)n * kNoAllocWords) != cudaSuccess) ||
-      cudaMemset(a->out, 0, sizeof(e13_check_out) * (size_t)n) != cudaSuccess ||
-      cudaMemcpy(a->in, in, sizeof(e13_check_in) * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess)
+  if ((!deep && cudaMemsetAsync(a->tapes, 0, sizeof(u32) * (size_t)n * kNoAllocWords, st) != cudaSuccess) ||
+      cudaMemsetAsync(a->out, 0, sizeof(e13_check_out) * (size_t)n, st) != cudaSuccess ||
+      cudaMemcpyAsync(a->in, in, sizeof(e13_check_in) * (size_t)n, cudaMemcpyHostToDevice, st) != cudaSuccess)
     return E13_ERR_CUDA;
   CheckParams P;
   P.n = n;
@@ -402,9 +413,10 @@ extern "C" int e13_check_noalloc(int device, const e13_check_in *in, int n, int 
   P.gtapes = a->tapes;
   P.in = a->in;
   P.out = a->out;
-  check_kernel<<<(n + nl - 1) / nl, nl, smem>>>(P);
-  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
-      cudaMemcpy(out, a->out, sizeof(e13_check_out) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+  check_kernel<<<(n + nl - 1) / nl, nl, smem, st>>>(P);
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(out, a->out, sizeof(e13_check_out) * (size_t)n, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
     return E13_ERR_CUDA;
   return E13_OK;
 }

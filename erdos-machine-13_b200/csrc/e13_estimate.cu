@@ -225,7 +225,9 @@ extern "C" void e13_ctx_note_run(e13_ctx *c, double ms, long long launches);
 
 extern "C" int e13_estimate(e13_ctx *ctx, const e13_job *job, int64_t probes, uint64_t seed, e13_estimate_out *out,
                             double *per_probe) {
-  if (!ctx || !job || !out || probes < 1) return E13_ERR_ARG;
+  // probe p draws from the stream that starts at mix(0x5EED0000 + p + (seed << 20)):
+  // from p = 2^20 on, the streams of seed would run into those of seed + 1
+  if (!ctx || !job || !out || probes < 1 || probes > E13_ESTIMATE_MAX_PROBES) return E13_ERR_ARG;
   if (job->nq < 1 || job->nq > 16) return E13_ERR_NQ;
   if (job->budget < 0) return E13_ERR_FMAX;
   for (int i = 0; i < 2 * job->nq; ++i)

@@ -178,6 +178,38 @@ void e13_default_tuning(e13_tuning *t) {
   t->stack_nodes = 0;
 }
 
+int e13_resolve_tuning(const e13_tuning *in, int serve, e13_tuning *out) {
+  if (!out) return E13_ERR_ARG;
+  e13_tuning t;
+  e13_default_tuning(&t);
+  if (serve) t.epoch_us = 10000; /* short epochs: jobs join and leave at every epoch boundary */
+  if (in) {
+    if (in->kernel != E13_KERNEL_PLAIN && in->kernel != E13_KERNEL_PERSISTENT) return E13_ERR_ARG;
+    if (in->run_skip != 0 && in->run_skip != 1) return E13_ERR_ARG;
+    if (in->block < 0 || in->slice < 0 || in->warp_stack < 0 || in->step_cap < 0 || in->batch < 0 ||
+        in->epoch_us < 0 || in->epochs_per_graph < 0 || in->pool_low_pct < 0 || in->stack_nodes < 0)
+      return E13_ERR_ARG;
+    t.kernel = in->kernel;
+    t.run_skip = in->run_skip;
+    if (in->block) t.block = in->block;
+    if (in->slice) t.slice = in->slice;
+    if (in->warp_stack) t.warp_stack = in->warp_stack;
+    if (in->step_cap) t.step_cap = in->step_cap;
+    if (in->batch) t.batch = in->batch;
+    if (in->epoch_us) t.epoch_us = in->epoch_us;
+    if (in->epochs_per_graph) t.epochs_per_graph = in->epochs_per_graph;
+    if (in->pool_low_pct) t.pool_low_pct = in->pool_low_pct;
+    if (in->stack_nodes) t.stack_nodes = in->stack_nodes;
+  }
+  if (serve) t.kernel = E13_KERNEL_PERSISTENT;
+  if (t.block < 64 || t.block > 768 || t.block % 32) return E13_ERR_ARG;
+  if (t.slice > 4096 || t.warp_stack > 4096) return E13_ERR_ARG;
+  if (t.epochs_per_graph > 64 || t.pool_low_pct > 100) return E13_ERR_ARG;
+  if (t.epoch_us > 60 * 1000 * 1000) return E13_ERR_ARG; /* one epoch at most a minute: checkpoints and stops stay timely */
+  *out = t;
+  return E13_OK;
+}
+
 /* ------------------------------------------------------------------ */
 /* checker text formats                                                */
 

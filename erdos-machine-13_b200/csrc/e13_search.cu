@@ -49,6 +49,7 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kKeySmemBytes = (kTapeCells + 64) * 8;
 constexpr long long kPoolNodes = 1LL << 18;  // donation pool: 256 Ki nodes (80 MiB)
 constexpr long long kWholeFrontier = 1LL << 62;  // persistent batch when e13_tuning::batch is 0
+constexpr long long kPoolWaitNs = 200000000;     // 200 ms: a donor publishes a claimed slot within microseconds
 
 // steps a lane gets between warp-level refill rounds is Params::slice
 
@@ -59,6 +60,7 @@ struct Params {
   int slice, step_cap, wdepth, pool_low, run_skip;
   long long out_cap, out_soft, surv_cap, pool_cap;
   long long epoch_ns;
+  long long wait_ns;         // persistent: limit of the wait for a claimed pool slot's data
   Node *stack, *out, *wstack, *pool;
   int *pool_ready;
   SurvRec *surv;
@@ -350,7 +352,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
                 // the donor claimed the slot before writing it; wait (bounded) for its data
                 const unsigned long long t0 = globaltimer();
                 while (*((volatile int *)&P.pool_ready[h]) != tag) {
-                  if (globaltimer() - t0 > 200000000ull) {
+                  if (globaltimer() - t0 > (unsigned long long)P.wait_ns) {
                     atomicOr(&ctl->error, kErrTimeout);
                     h = -1;
                     break;
@@ -776,6 +778,17 @@ static int cuda_fail(cudaError_t e, const char *what) {
     if (cuda_fail((x), #x)) return E13_ERR_CUDA; \
   } while (0)
 
+// Host<->device copies on the context's stream, counted in its statistics
+// (the bytes an end-to-end caller moves across PCIe/C2C per search).
+static cudaError_t h2d(e13_ctx *c, void *dst, const void *src, size_t bytes) {
+  c->stats.h2d_bytes += (int64_t)bytes;
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+}
+static cudaError_t d2h(e13_ctx *c, void *dst, const void *src, size_t bytes) {
+  c->stats.d2h_bytes += (int64_t)bytes;
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+}
+
 static int ensure_consts(e13_ctx *c) {
   if (c->consts_ready) return E13_OK;
   if (upload_filter_tables() != cudaSuccess) return E13_ERR_CUDA;
@@ -880,6 +893,39 @@ static void decode_survivor(const SurvRec &r, int nq, e13_survivor *s) {
   s->steps = r.t;
 }
 
+// Kernel parameters of a search or serve session over the context's buffers.
+// dump_room: frontier nodes the warps may write when an epoch ends.
+static Params make_params(const e13_ctx *c, const e13_tuning &tu, int nq, long long nwarps, long long dump_room) {
+  Params P;
+  memset(&P, 0, sizeof P);
+  P.jobs = c->d_jobs;
+  P.jobcnt = c->d_jobcnt;
+  P.nq = nq;
+  P.slice = tu.slice;
+  P.run_skip = tu.run_skip ? 1 : 0;
+  P.step_cap = tu.step_cap;
+  P.wdepth = tu.warp_stack;
+  P.pool_low = (int)std::max<long long>(1, nwarps * tu.pool_low_pct / 100);
+  P.pool_cap = c->pool_cap;
+  P.pool = c->pool;
+  P.pool_ready = c->pool_ready;
+  P.out_cap = c->out_cap;
+  P.out_soft = c->out_cap - dump_room - 1024;
+  P.surv_cap = c->surv_cap;
+  P.epoch_ns = (long long)tu.epoch_us * 1000LL;
+  P.wait_ns = kPoolWaitNs;
+  P.stack = c->stack;
+  P.out = c->out;
+  P.wstack = c->wstack;
+  P.surv = c->surv;
+  P.ctl = c->ctl;
+  return P;
+}
+
+static size_t search_smem(int block) {
+  return kKeySmemBytes + (size_t)(kTapeWords + 16) * block * 4 + (size_t)(block / 32) * sizeof(Node);
+}
+
 // ------------------------------------------------------------------------
 // checkpoint files of one search (e13_search_resumable)
 //
@@ -934,7 +980,7 @@ int ckpt_save(e13_ctx *c, const e13_job *job, const e13_checkpoint *ck, int slot
   std::vector<Node> buf((size_t)std::min(std::max(top, 1LL), kCkptChunk));
   for (long long o = 0; o < top; o += kCkptChunk) {
     const long long n = std::min(kCkptChunk, top - o);
-    if (cudaMemcpyAsync(buf.data(), c->stack + o, sizeof(Node) * n, cudaMemcpyDeviceToHost, c->stream) !=
+    if (d2h(c, buf.data(), c->stack + o, sizeof(Node) * n) !=
             cudaSuccess ||
         cudaStreamSynchronize(c->stream) != cudaSuccess) {
       fclose(f);
@@ -950,8 +996,8 @@ int ckpt_save(e13_ctx *c, const e13_job *job, const e13_checkpoint *ck, int slot
   unsigned long long cnt[kJobCounters];
   const unsigned long long nrec = std::min<unsigned long long>(h.nsurv, (unsigned long long)c->surv_cap);
   std::vector<SurvRec> recs((size_t)nrec);
-  CK(cudaMemcpyAsync(cnt, c->d_jobcnt, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
-  if (nrec) CK(cudaMemcpyAsync(recs.data(), c->surv, sizeof(SurvRec) * nrec, cudaMemcpyDeviceToHost, c->stream));
+  CK(d2h(c, cnt, c->d_jobcnt, sizeof cnt));
+  if (nrec) CK(d2h(c, recs.data(), c->surv, sizeof(SurvRec) * nrec));
   CK(cudaStreamSynchronize(c->stream));
   CkptHeader hd;
   memset(&hd, 0, sizeof hd);
@@ -1028,7 +1074,7 @@ int ckpt_load(e13_ctx *c, const e13_job *job, const e13_checkpoint *ck, long lon
       fclose(f);
       return E13_ERR_CKPT;
     }
-    if (cudaMemcpyAsync(c->stack + o, buf.data(), sizeof(Node) * n, cudaMemcpyHostToDevice, c->stream) !=
+    if (h2d(c, c->stack + o, buf.data(), sizeof(Node) * n) !=
             cudaSuccess ||
         cudaStreamSynchronize(c->stream) != cudaSuccess) {
       fclose(f);
@@ -1045,9 +1091,9 @@ int ckpt_load(e13_ctx *c, const e13_job *job, const e13_checkpoint *ck, long lon
   c->ctl_host->peak = std::max<long long>(hd.peak, hd.top);
   c->ctl_host->launches = (int)hd.launches;
   c->ctl_host->nsurv = hd.nsurv;
-  CK(cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(c->d_jobcnt, cnt, sizeof cnt, cudaMemcpyHostToDevice, c->stream));
-  if (hd.nrec) CK(cudaMemcpyAsync(c->surv, recs.data(), sizeof(SurvRec) * hd.nrec, cudaMemcpyHostToDevice, c->stream));
+  CK(h2d(c, c->ctl, c->ctl_host, sizeof(Ctl)));
+  CK(h2d(c, c->d_jobcnt, cnt, sizeof cnt));
+  if (hd.nrec) CK(h2d(c, c->surv, recs.data(), sizeof(SurvRec) * hd.nrec));
   CK(cudaStreamSynchronize(c->stream));
   *prior_wall = hd.wall;
   return E13_OK;
@@ -1120,22 +1166,7 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
   for (int i = 0; i < 2 * job->nq; ++i)
     if (job->tab[i] < E13_FREE || (job->tab[i] >= 0 && (job->tab[i] >> 2) >= job->nq)) return E13_ERR_ARG;
   e13_tuning tu;
-  e13_default_tuning(&tu);
-  if (tuning) {
-    if (tuning->kernel == E13_KERNEL_PLAIN || tuning->kernel == E13_KERNEL_PERSISTENT) tu.kernel = tuning->kernel;
-    if (tuning->block) tu.block = tuning->block;
-    if (tuning->slice) tu.slice = tuning->slice;
-    if (tuning->warp_stack) tu.warp_stack = tuning->warp_stack;
-    if (tuning->step_cap) tu.step_cap = tuning->step_cap;
-    if (tuning->batch) tu.batch = tuning->batch;
-    if (tuning->epoch_us) tu.epoch_us = tuning->epoch_us;
-    if (tuning->epochs_per_graph) tu.epochs_per_graph = tuning->epochs_per_graph;
-    if (tuning->pool_low_pct) tu.pool_low_pct = tuning->pool_low_pct;
-    tu.run_skip = tuning->run_skip;
-    if (tuning->stack_nodes) tu.stack_nodes = tuning->stack_nodes;
-  }
-  if (tu.block < 64 || tu.block > 768 || tu.block % 32) return E13_ERR_ARG;
-  if (tu.slice < 1 || tu.warp_stack < 1 || tu.warp_stack > 4096) return E13_ERR_ARG;
+  if (e13_resolve_tuning(tuning, 0, &tu) != E13_OK) return E13_ERR_ARG;
   CK(cudaSetDevice(c->device));
   int rc = ensure_consts(c);
   if (rc) return rc;
@@ -1157,6 +1188,9 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
     out_nodes = batch_max * (4LL * job->nq + 1) + nwarps * 32 + 1024;
   }
   if ((rc = grow(&c->stack, &c->stack_cap, stack_nodes))) return rc;
+  // the frontier capacity of this search: exactly what the tuning asks for,
+  // else all that the context holds (a larger stack left by a serve session)
+  const long long cap = tu.stack_nodes > 0 ? tu.stack_nodes : c->stack_cap;
   if ((rc = grow(&c->out, &c->out_cap, out_nodes))) return rc;
   if (persist && (rc = grow(&c->wstack, &c->wstack_nodes, nwarps * tu.warp_stack))) return rc;
   if (persist && (rc = grow(&c->pool, &c->pool_cap, kPoolNodes))) return rc;
@@ -1169,31 +1203,11 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
   jp[0].nv = 4 * job->nq;
   jp[0].sym_lo = job->sym_lo;
   jp[0].sym_hi = job->sym_hi;
-  CK(cudaMemcpyAsync(c->d_jobs, jp, sizeof jp, cudaMemcpyHostToDevice, c->stream));
+  CK(h2d(c, c->d_jobs, jp, sizeof jp));
   CK(cudaMemsetAsync(c->d_jobcnt, 0, sizeof(unsigned long long) * kMaxJobs * kJobCounters, c->stream));
-  Params P;
-  P.jobs = c->d_jobs;
-  P.jobcnt = c->d_jobcnt;
-  P.nq = job->nq;
-  P.slice = tu.slice;
-  P.run_skip = tu.run_skip ? 1 : 0;
-  P.step_cap = tu.step_cap;
-  P.wdepth = tu.warp_stack;
-  P.pool_low = (int)std::max<long long>(1, nwarps * tu.pool_low_pct / 100);
-  P.pool_cap = c->pool_cap;
-  P.pool = c->pool;
-  P.pool_ready = c->pool_ready;
-  P.out_cap = c->out_cap;
-  P.out_soft = c->out_cap - dump_room - 1024;
-  P.surv_cap = c->surv_cap;
-  P.epoch_ns = (long long)tu.epoch_us * 1000LL;
-  P.stack = c->stack;
-  P.out = c->out;
-  P.wstack = c->wstack;
-  P.surv = c->surv;
-  P.ctl = c->ctl;
+  Params P = make_params(c, tu, job->nq, nwarps, dump_room);
 
-  const size_t smem = kKeySmemBytes + (size_t)(kTapeWords + 16) * tu.block * 4 + (size_t)(tu.block / 32) * sizeof(Node);
+  const size_t smem = search_smem(tu.block);
   if (persist) CK(cudaFuncSetAttribute(search_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   else CK(cudaFuncSetAttribute(search_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
@@ -1204,10 +1218,10 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
   c->ctl_host->top = 1;
   c->ctl_host->batch = 1;
   c->ctl_host->peak = 1;
-  CK(cudaMemcpyAsync(c->stack, &root, sizeof root, cudaMemcpyHostToDevice, c->stream));
+  CK(h2d(c, c->stack, &root, sizeof root));
   // pool slots carry the tag of the launch that wrote them; tags restart with every search
   if (persist) CK(cudaMemsetAsync(c->pool_ready, 0, sizeof(int) * (size_t)c->pool_ready_cap, c->stream));
-  CK(cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+  CK(h2d(c, c->ctl, c->ctl_host, sizeof(Ctl)));
 
   // checkpoints: resume from the last complete slot, then save into the other one
   double prior_wall = 0.0;
@@ -1218,7 +1232,7 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
     if (file_exists(clk.stop_file)) remove(clk.stop_file.c_str());  // left from the last clean stop
     if (file_exists(ck->path)) {
       int loaded = 0;
-      if ((rc = ckpt_load(c, job, ck, batch_max, c->stack_cap - out_nodes, &loaded, &prior_wall))) return rc;
+      if ((rc = ckpt_load(c, job, ck, batch_max, cap - out_nodes, &loaded, &prior_wall))) return rc;
       slot = loaded ^ 1;
     }
   }
@@ -1264,12 +1278,12 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
       S.out = c->out;
       S.out_cap = c->out_cap;
       search_kernel<false><<<blocks, tu.block, smem, c->stream>>>(S);
-      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, c->stack_cap);
-      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, kWholeFrontier, c->pool_cap);
+      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, cap);
+      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, cap, kWholeFrontier, c->pool_cap);
       launches += 3;
       search_launches += 1;
       CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(c->ctl_host, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+      CK(d2h(c, c->ctl_host, c->ctl, sizeof(Ctl)));
       CK(cudaStreamSynchronize(c->stream));
       if (c->ctl_host->error) return E13_ERR_OVERFLOW;
       top = c->ctl_host->top;
@@ -1277,7 +1291,7 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
     // the deal
     std::vector<Node> nodes((size_t)top);
     if (top > 0)
-      CK(cudaMemcpyAsync(nodes.data(), c->stack, sizeof(Node) * (size_t)top, cudaMemcpyDeviceToHost, c->stream));
+      CK(d2h(c, nodes.data(), c->stack, sizeof(Node) * (size_t)top));
     CK(cudaStreamSynchronize(c->stream));
     std::vector<std::pair<ShardKey, long long>> order((size_t)top);
     for (long long i = 0; i < top; ++i) order[(size_t)i] = {shard_key(nodes[(size_t)i]), i};
@@ -1286,14 +1300,14 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
     std::vector<Node> mine;
     for (long long i = shard; i < top; i += nshards) mine.push_back(nodes[(size_t)order[(size_t)i].second]);
     if (!mine.empty())
-      CK(cudaMemcpyAsync(c->stack, mine.data(), sizeof(Node) * mine.size(), cudaMemcpyHostToDevice, c->stream));
+      CK(h2d(c, c->stack, mine.data(), sizeof(Node) * mine.size()));
     c->ctl_host->top = (long long)mine.size();
     c->ctl_host->batch = std::min<long long>((long long)mine.size(), batch_max);
     if (shard != 0) {
       c->ctl_host->nsurv = 0;
       CK(cudaMemsetAsync(c->d_jobcnt, 0, sizeof(unsigned long long) * kMaxJobs * kJobCounters, c->stream));
     }
-    CK(cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+    CK(h2d(c, c->ctl, c->ctl_host, sizeof(Ctl)));
     CK(cudaStreamSynchronize(c->stream));
     // the split may have grown the output buffer: the main phase uses the new one
     P.out = c->out;
@@ -1306,8 +1320,8 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     for (int e = 0; e < tu.epochs_per_graph; ++e) {
       search_kernel<true><<<blocks, tu.block, smem, c->stream>>>(P);
-      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, c->stack_cap);
-      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, batch_max, c->pool_cap);
+      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, cap);
+      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, cap, batch_max, c->pool_cap);
     }
     CK(cudaStreamEndCapture(c->stream, &graph));
     CK(cudaGraphInstantiate(&exec, graph, 0));
@@ -1315,17 +1329,17 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
       CK(cudaGraphLaunch(exec, c->stream));
       launches += 3LL * tu.epochs_per_graph;
       search_launches += tu.epochs_per_graph;
-      CK(cudaMemcpyAsync(c->ctl_host, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+      CK(d2h(c, c->ctl_host, c->ctl, sizeof(Ctl)));
       CK(cudaStreamSynchronize(c->stream));
       if (c->ctl_host->error) {
         err = (c->ctl_host->error & kErrTimeout) ? E13_ERR_TIMEOUT : E13_ERR_OVERFLOW;
         break;
       }
-      if (c->ctl_host->top > c->stack_cap - (long long)out_nodes) {
+      if (c->ctl_host->top == 0) break;
+      if (c->ctl_host->top > cap - (long long)out_nodes) {  // the next epoch's outputs might not fit
         err = E13_ERR_OVERFLOW;
         break;
       }
-      if (c->ctl_host->top == 0) break;
       if (checkpoint_step(err)) break;
     }
     cudaGraphExecDestroy(exec);
@@ -1333,22 +1347,22 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
   } else {
     for (;;) {
       search_kernel<false><<<blocks, tu.block, smem, c->stream>>>(P);
-      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, c->stack_cap);
-      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, batch_max, c->pool_cap);
+      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, cap);
+      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, cap, batch_max, c->pool_cap);
       launches += 3;
       search_launches += 1;
       CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(c->ctl_host, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+      CK(d2h(c, c->ctl_host, c->ctl, sizeof(Ctl)));
       CK(cudaStreamSynchronize(c->stream));
       if (c->ctl_host->error) {
         err = E13_ERR_OVERFLOW;
         break;
       }
-      if (c->ctl_host->top > c->stack_cap - (long long)out_nodes) {
+      if (c->ctl_host->top == 0) break;
+      if (c->ctl_host->top > cap - (long long)out_nodes) {  // the next launch's outputs might not fit
         err = E13_ERR_OVERFLOW;
         break;
       }
-      if (c->ctl_host->top == 0) break;
       if (checkpoint_step(err)) break;
     }
   }
@@ -1371,7 +1385,8 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
   if (err) return err;
 
   const Ctl &h = *c->ctl_host;
-  CK(cudaMemcpy(c->h_jobbuf, c->d_jobcnt, sizeof(unsigned long long) * kJobCounters, cudaMemcpyDeviceToHost));
+  CK(d2h(c, c->h_jobbuf, c->d_jobcnt, sizeof(unsigned long long) * kJobCounters));
+  CK(cudaStreamSynchronize(c->stream));
   memset(counts, 0, sizeof *counts);
   counts->leaves = c->h_jobbuf[0];
   counts->steps = c->h_jobbuf[1];
@@ -1386,7 +1401,7 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
       survivor_read_masks<<<(unsigned)((ncopy + 31) / 32), 32, 0, c->stream>>>(c->surv, ncopy);
       CK(cudaGetLastError());
     }
-    CK(cudaMemcpyAsync(recs.data(), c->surv, sizeof(SurvRec) * (size_t)ncopy, cudaMemcpyDeviceToHost, c->stream));
+    CK(d2h(c, recs.data(), c->surv, sizeof(SurvRec) * (size_t)ncopy));
     CK(cudaStreamSynchronize(c->stream));
     for (long long i = 0; i < ncopy; ++i) decode_survivor(recs[(size_t)i], job->nq, &surv[i]);
   }
@@ -1425,17 +1440,61 @@ extern "C" int e13_run_full(e13_ctx *c, const int32_t *tabs, int n, int nq, int6
   long long *d_out = nullptr;
   CK(cudaMalloc(&d_tabs, sizeof(int) * E13_MAXCELLS * (size_t)n));
   CK(cudaMalloc(&d_out, sizeof(long long) * 7 * (size_t)n));
-  CK(cudaMemcpyAsync(d_tabs, tabs, sizeof(int) * E13_MAXCELLS * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+  CK(h2d(c, d_tabs, tabs, sizeof(int) * E13_MAXCELLS * (size_t)n));
   const int bd = 256;
   const size_t smem = kKeySmemBytes + (size_t)(kTapeWords + 16) * bd * 4;
   CK(cudaFuncSetAttribute(run_full_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   run_full_kernel<<<(n + bd - 1) / bd, bd, smem, c->stream>>>(d_tabs, n, nq, d_out);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(out, d_out, sizeof(long long) * 7 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  CK(d2h(c, out, d_out, sizeof(long long) * 7 * (size_t)n));
   CK(cudaStreamSynchronize(c->stream));
   cudaFree(d_tabs);
   cudaFree(d_out);
   return E13_OK;
+}
+
+// One epoch of the persistent kernel in which the donation pool holds one
+// claimed slot whose donor never publishes it: the warp that claims it waits
+// for the slot's ready tag, gives up after wait_us, and flags kErrTimeout.
+// Nothing else is on the frontier, so the epoch then ends.  The slot's data is
+// never read (the claim is dropped when the wait runs out).
+extern "C" int e13_selftest_pool_wait(e13_ctx *c, int32_t wait_us) {
+  if (!c || wait_us < 1 || wait_us > 1000000) return E13_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  int rc = ensure_consts(c);
+  if (rc) return rc;
+  e13_tuning tu;
+  e13_resolve_tuning(nullptr, 0, &tu);
+  const long long nwarps = (long long)c->nsm * tu.block / 32;
+  const long long dump_room = nwarps * (32 + tu.warp_stack);
+  if ((rc = grow(&c->stack, &c->stack_cap, 1024))) return rc;
+  if ((rc = grow(&c->out, &c->out_cap, 2 * dump_room + 65536))) return rc;
+  if ((rc = grow(&c->wstack, &c->wstack_nodes, nwarps * tu.warp_stack))) return rc;
+  if ((rc = grow(&c->pool, &c->pool_cap, kPoolNodes))) return rc;
+  if ((rc = grow(&c->pool_ready, &c->pool_ready_cap, kPoolNodes))) return rc;
+  if ((rc = grow(&c->surv, &c->surv_cap, 1024))) return rc;
+  Params P = make_params(c, tu, 16, nwarps, dump_room);
+  P.wait_ns = (long long)wait_us * 1000LL;
+  const size_t smem = search_smem(tu.block);
+  CK(cudaFuncSetAttribute(search_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  JobParam jp[kMaxJobs];
+  memset(jp, 0, sizeof jp);
+  CK(h2d(c, c->d_jobs, jp, sizeof jp));
+  CK(cudaMemsetAsync(c->d_jobcnt, 0, sizeof(unsigned long long) * kMaxJobs * kJobCounters, c->stream));
+  // ready tags 0; the launch's tag is launches + 1 = 1, so slot 0 never looks published
+  CK(cudaMemsetAsync(c->pool_ready, 0, sizeof(int) * (size_t)c->pool_ready_cap, c->stream));
+  memset(c->ctl_host, 0, sizeof(Ctl));
+  c->ctl_host->pool_tail = 1;  // slot 0 donated (claimable), its data never written
+  CK(h2d(c, c->ctl, c->ctl_host, sizeof(Ctl)));
+  search_kernel<true><<<c->nsm, tu.block, smem, c->stream>>>(P);
+  move_outputs<<<c->nsm * 4, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, c->stack_cap);
+  finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, kWholeFrontier, c->pool_cap);
+  CK(cudaGetLastError());
+  CK(d2h(c, c->ctl_host, c->ctl, sizeof(Ctl)));
+  CK(cudaStreamSynchronize(c->stream));
+  const int err = c->ctl_host->error;
+  if (err & kErrTimeout) return E13_ERR_TIMEOUT;
+  return err ? E13_ERR_OVERFLOW : E13_OK;
 }
 
 // ------------------------------------------------------------------------
@@ -1498,14 +1557,24 @@ extern "C" int e13_autotune(e13_ctx *c, const e13_job *job, const e13_tuning *st
 #include <memory>
 #include <unordered_map>
 
+extern "C" int e13_estimate(e13_ctx *ctx, const e13_job *job, int64_t probes, uint64_t seed, e13_estimate_out *out,
+                            double *per_probe);
+
 namespace {
+
+constexpr int64_t kAdmitProbes = 64;  // Knuth probes behind a job's frontier reservation
 
 struct ServeJob {
   int64_t id;
   e13_job job;
   double t_submit, t_start;
   int slot;
+  long long reserve;                    // frontier nodes reserved while it runs
   std::vector<e13_survivor> surv;
+  // swapped out: its frontier nodes and counters, put back on re-admission
+  bool swapped = false;
+  std::vector<Node> saved;
+  unsigned long long saved_cnt[kJobCounters];
 };
 
 double wall_seconds() {
@@ -1520,7 +1589,7 @@ struct e13_serve {
   e13_tuning tu;
   Params P;
   size_t smem;
-  long long batch_max, out_nodes, reserve;
+  long long batch_max, out_nodes, fixed_reserve, cap, large_reserve;
   std::deque<std::unique_ptr<ServeJob>> queue;
   std::unique_ptr<ServeJob> slot_job[kMaxJobs];
   std::unordered_map<int64_t, std::vector<e13_survivor>> finished_surv;
@@ -1529,7 +1598,7 @@ struct e13_serve {
   bool surv_overflow;
   double t0;
   double device_ms;
-  long long epochs;
+  long long epochs, evictions;
   // frontier order between epochs: a second stack buffer, the group starts
   Node *alt = nullptr;
   long long alt_cap = 0;
@@ -1543,23 +1612,10 @@ struct e13_serve {
 };
 
 extern "C" int e13_serve_create(e13_ctx *c, const e13_tuning *tuning, int64_t reserve_nodes, e13_serve **out) {
-  if (!c || !out) return E13_ERR_ARG;
+  if (!c || !out || reserve_nodes < 0) return E13_ERR_ARG;
   *out = nullptr;
   e13_tuning tu;
-  e13_default_tuning(&tu);
-  tu.epoch_us = 10000;  // short epochs: new jobs join, and finished ones leave, at every epoch boundary
-  if (tuning) {
-    if (tuning->block) tu.block = tuning->block;
-    if (tuning->slice) tu.slice = tuning->slice;
-    if (tuning->warp_stack) tu.warp_stack = tuning->warp_stack;
-    if (tuning->epoch_us) tu.epoch_us = tuning->epoch_us;
-    if (tuning->pool_low_pct) tu.pool_low_pct = tuning->pool_low_pct;
-    if (tuning->batch) tu.batch = tuning->batch;
-    tu.run_skip = tuning->run_skip;
-    if (tuning->stack_nodes) tu.stack_nodes = tuning->stack_nodes;
-  }
-  tu.kernel = E13_KERNEL_PERSISTENT;
-  if (tu.block < 64 || tu.block > 768 || tu.block % 32 || tu.slice < 1 || tu.warp_stack < 1) return E13_ERR_ARG;
+  if (e13_resolve_tuning(tuning, 1, &tu) != E13_OK) return E13_ERR_ARG;
   CK(cudaSetDevice(c->device));
   int rc = ensure_consts(c);
   if (rc) return rc;
@@ -1570,44 +1626,28 @@ extern "C" int e13_serve_create(e13_ctx *c, const e13_tuning *tuning, int64_t re
   const long long dump_room = nwarps * (32 + tu.warp_stack);
   s->batch_max = tu.batch > 0 ? tu.batch : kWholeFrontier;
   s->out_nodes = 2 * dump_room + 65536;
-  s->reserve = reserve_nodes > 0 ? reserve_nodes : (1LL << 16);
+  s->fixed_reserve = reserve_nodes;
+  // a job too big for its estimate to bound its frontier reserves what one
+  // epoch's dump of every warp can leave behind
+  s->large_reserve = dump_room;
   // serving keeps many frontiers resident: 16 Mi nodes (5 GB) by default
   const long long stack_nodes = tu.stack_nodes > 0 ? tu.stack_nodes : (16LL << 20);
   if ((rc = grow(&c->stack, &c->stack_cap, stack_nodes))) return rc;
+  s->cap = tu.stack_nodes > 0 ? tu.stack_nodes : c->stack_cap;
   if ((rc = grow(&c->out, &c->out_cap, s->out_nodes))) return rc;
   if ((rc = grow(&c->wstack, &c->wstack_nodes, nwarps * tu.warp_stack))) return rc;
   if ((rc = grow(&c->pool, &c->pool_cap, kPoolNodes))) return rc;
   if ((rc = grow(&c->pool_ready, &c->pool_ready_cap, kPoolNodes))) return rc;
   if ((rc = grow(&c->surv, &c->surv_cap, 1LL << 20))) return rc;
   memset(s->jp, 0, sizeof s->jp);
-  Params &P = s->P;
-  P.jobs = c->d_jobs;
-  P.jobcnt = c->d_jobcnt;
-  P.nq = 16;
-  P.slice = tu.slice;
-  P.run_skip = tu.run_skip ? 1 : 0;
-  P.step_cap = tu.step_cap;
-  P.wdepth = tu.warp_stack;
-  P.pool_low = (int)std::max<long long>(1, nwarps * tu.pool_low_pct / 100);
-  P.pool_cap = c->pool_cap;
-  P.pool = c->pool;
-  P.pool_ready = c->pool_ready;
-  P.out_cap = c->out_cap;
-  P.out_soft = c->out_cap - dump_room - 1024;
-  P.surv_cap = c->surv_cap;
-  P.epoch_ns = (long long)tu.epoch_us * 1000LL;
-  P.stack = c->stack;
-  P.out = c->out;
-  P.wstack = c->wstack;
-  P.surv = c->surv;
-  P.ctl = c->ctl;
-  s->smem = kKeySmemBytes + (size_t)(kTapeWords + 16) * tu.block * 4 + (size_t)(tu.block / 32) * sizeof(Node);
+  s->P = make_params(c, tu, 16, nwarps, dump_room);
+  s->smem = search_smem(tu.block);
   CK(cudaFuncSetAttribute(search_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem));
   memset(c->ctl_host, 0, sizeof(Ctl));
-  CK(cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+  CK(h2d(c, c->ctl, c->ctl_host, sizeof(Ctl)));
   CK(cudaMemsetAsync(c->pool_ready, 0, sizeof(int) * (size_t)c->pool_ready_cap, c->stream));
   CK(cudaMemsetAsync(c->d_jobcnt, 0, sizeof(unsigned long long) * kMaxJobs * kJobCounters, c->stream));
-  CK(cudaMemcpyAsync(c->d_jobs, s->jp, sizeof s->jp, cudaMemcpyHostToDevice, c->stream));
+  CK(h2d(c, c->d_jobs, s->jp, sizeof s->jp));
   CK(cudaMalloc(&s->alt, sizeof(Node) * (size_t)c->stack_cap));
   s->alt_cap = c->stack_cap;
   CK(cudaMalloc(&s->d_fill, sizeof(unsigned long long) * kMaxJobs));
@@ -1634,6 +1674,19 @@ extern "C" int e13_serve_submit(e13_serve *s, const e13_job *job, int64_t id, do
   j->t_submit = t_submit >= 0 ? t_submit : e13_serve_clock(s);
   j->t_start = -1;
   j->slot = -1;
+  if (s->fixed_reserve > 0) {
+    j->reserve = s->fixed_reserve;
+  } else {
+    // the frontier of a search never holds more machines than its tree has
+    // nodes and leaves: a job the estimate puts below one epoch's dump
+    // reserves twice its estimate, a larger one the dump bound
+    e13_estimate_out est;
+    const int rc = e13_estimate(s->c, job, kAdmitProbes, 0, &est, nullptr);
+    if (rc) return rc;
+    const double tree = est.mean[0] + est.mean[1];
+    j->reserve = tree * 2.0 < (double)s->large_reserve ? std::max<long long>(64, (long long)(tree * 2.0) + 1)
+                                                       : s->large_reserve;
+  }
   s->queue.push_back(std::move(j));
   return E13_OK;
 }
@@ -1643,6 +1696,53 @@ extern "C" int64_t e13_serve_pending(const e13_serve *s) {
   int64_t n = (int64_t)s->queue.size();
   for (int k = 0; k < kMaxJobs; ++k) n += s->slot_job[k] ? 1 : 0;
   return n;
+}
+
+namespace {
+
+void fill_result(e13_serve_result &r, const ServeJob &j, const unsigned long long *cnt, int status, double tdone) {
+  memset(&r, 0, sizeof r);
+  r.id = j.id;
+  r.counts.leaves = cnt[0];
+  r.counts.steps = cnt[1];
+  for (int h = 0; h <= E13_STAGES; ++h) r.counts.hist[h] = cnt[2 + h];
+  r.counts.survivors = (uint64_t)j.surv.size();
+  r.nsurv = (int32_t)j.surv.size();
+  r.status = status;
+  r.t_submit = j.t_submit;
+  r.t_start = j.t_start;
+  r.t_done = tdone;
+}
+
+}  // namespace
+
+// Regroups the frontier by job into s->alt, groups laid out bottom to top in
+// `order` (the last one ends on top), and makes it the frontier.
+static int regroup(e13_serve *s, const int *order, int n, const unsigned long long *nodes) {
+  e13_ctx *c = s->c;
+  unsigned long long off = 0;
+  memset(s->fill, 0, sizeof s->fill);
+  for (int i = 0; i < n; ++i) {
+    s->fill[order[i]] = off;
+    off += nodes[order[i]];
+  }
+  CK(h2d(c, s->d_fill, s->fill, sizeof s->fill));
+  order_by_job<<<c->nsm * 4, 256, 0, c->stream>>>(c->ctl, c->stack, s->alt, s->d_fill, s->alt_cap);
+  CK(cudaGetLastError());
+  std::swap(c->stack, s->alt);
+  s->P.stack = c->stack;
+  c->stats.launches += 1;
+  return E13_OK;
+}
+
+// Sets the frontier's size on the device (Ctl::top, Ctl::batch) and here.
+static int set_top(e13_serve *s, long long top) {
+  e13_ctx *c = s->c;
+  c->ctl_host->top = top;
+  c->ctl_host->batch = std::min(top, s->batch_max);
+  long long tb[2] = {top, c->ctl_host->batch};
+  CK(h2d(c, c->ctl, tb, sizeof tb));  // Ctl::top, Ctl::batch
+  return E13_OK;
 }
 
 extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int *ndone) {
@@ -1655,7 +1755,7 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
   long long launches = 0;
   // 0. the frontier in the order the last step chose (fewest live nodes on top)
   if (s->reorder && s->alt_cap >= c->stack_cap) {
-    CK(cudaMemcpyAsync(s->d_fill, s->fill, sizeof s->fill, cudaMemcpyHostToDevice, c->stream));
+    CK(h2d(c, s->d_fill, s->fill, sizeof s->fill));
     order_by_job<<<c->nsm * 4, 256, 0, c->stream>>>(c->ctl, c->stack, s->alt, s->d_fill, s->alt_cap);
     CK(cudaGetLastError());
     std::swap(c->stack, s->alt);
@@ -1663,57 +1763,76 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
     ++launches;
   }
   s->reorder = false;
-  // 1. admission: a free slot, the job's arrival time passed, and frontier room
-  //    for every running job's reservation plus this one
+  // 1. admission, first come first served: a free slot, the job's arrival
+  //    time passed, and room for every running job's reservation plus its own
+  //    (a job alone is always admitted).  A swapped-out job comes back with its
+  //    frontier nodes and counters.
   int running = 0;
-  for (int k = 0; k < kMaxJobs; ++k) running += s->slot_job[k] ? 1 : 0;
+  long long reserved = 0;
+  for (int k = 0; k < kMaxJobs; ++k)
+    if (s->slot_job[k]) {
+      ++running;
+      reserved += s->slot_job[k]->reserve;
+    }
   long long top = c->ctl_host->top;
-  std::vector<Node> roots;
+  bool pushed = false;
   while (!s->queue.empty() && s->queue.front()->t_submit <= now) {
     int slot = -1;
     for (int k = 0; k < kMaxJobs && slot < 0; ++k)
       if (!s->slot_job[k]) slot = k;
     if (slot < 0) break;
-    const long long need = top + (long long)roots.size() + s->reserve * (running + 1) + s->out_nodes;
-    if (need > c->stack_cap) break;
+    ServeJob &q = *s->queue.front();
+    const long long start_nodes = q.swapped ? (long long)q.saved.size() : 1;
+    if (running > 0 && (reserved + q.reserve + s->out_nodes > s->cap || top + start_nodes + s->out_nodes > s->cap))
+      break;
+    if (top + start_nodes > s->cap) break;  // cannot happen when nothing runs (the frontier is empty then)
     std::unique_ptr<ServeJob> j = std::move(s->queue.front());
     s->queue.pop_front();
     j->slot = slot;
-    j->t_start = now;
+    if (j->t_start < 0) j->t_start = now;
     s->jp[slot].nv = 4 * j->job.nq;
     s->jp[slot].sym_lo = j->job.sym_lo;
     s->jp[slot].sym_hi = j->job.sym_hi;
-    Node root;
-    build_root(&j->job, slot, &root, s->tu.run_skip != 0, true);
-    roots.push_back(root);
-    CK(cudaMemsetAsync(c->d_jobcnt + (size_t)slot * kJobCounters, 0, sizeof(unsigned long long) * kJobCounters,
-                       c->stream));
+    if (j->swapped) {
+      for (Node &nd : j->saved) nd.job = (unsigned char)slot;
+      if (!j->saved.empty()) CK(h2d(c, c->stack + top, j->saved.data(), sizeof(Node) * j->saved.size()));
+      CK(h2d(c, c->d_jobcnt + (size_t)slot * kJobCounters, j->saved_cnt, sizeof j->saved_cnt));
+      CK(cudaStreamSynchronize(c->stream));  // the host buffer goes away next
+      top += (long long)j->saved.size();
+      std::vector<Node>().swap(j->saved);
+      j->swapped = false;
+    } else {
+      Node root;
+      build_root(&j->job, slot, &root, s->tu.run_skip != 0, true);
+      CK(h2d(c, c->stack + top, &root, sizeof root));
+      CK(cudaStreamSynchronize(c->stream));
+      CK(cudaMemsetAsync(c->d_jobcnt + (size_t)slot * kJobCounters, 0, sizeof(unsigned long long) * kJobCounters,
+                         c->stream));
+      top += 1;
+    }
+    reserved += j->reserve;
     s->slot_job[slot] = std::move(j);
     ++running;
+    pushed = true;
   }
-  if (!roots.empty()) {
-    CK(cudaMemcpyAsync(c->stack + top, roots.data(), sizeof(Node) * roots.size(), cudaMemcpyHostToDevice, c->stream));
-    top += (long long)roots.size();
-    long long tb[2] = {top, std::min(top, s->batch_max)};
-    CK(cudaMemcpyAsync(c->ctl, tb, sizeof tb, cudaMemcpyHostToDevice, c->stream));  // Ctl::top, Ctl::batch
-    CK(cudaMemcpyAsync(c->d_jobs, s->jp, sizeof s->jp, cudaMemcpyHostToDevice, c->stream));
-    c->ctl_host->top = top;
+  if (pushed) {
+    int rc;
+    if ((rc = set_top(s, top))) return rc;
+    CK(h2d(c, c->d_jobs, s->jp, sizeof s->jp));
   }
   if (running == 0) return E13_OK;
   // 2. one epoch of the persistent kernel, then the live nodes of every job
   launches += 4;
   search_kernel<true><<<c->nsm, s->tu.block, s->smem, c->stream>>>(s->P);
-  move_outputs<<<c->nsm * 4, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, c->stack_cap);
-  finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, c->stack_cap, s->batch_max, c->pool_cap);
+  move_outputs<<<c->nsm * 4, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, s->cap);
+  finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, s->cap, s->batch_max, c->pool_cap);
   CK(cudaMemsetAsync(c->d_jobnodes, 0, sizeof(unsigned long long) * kMaxJobs, c->stream));
   count_job_nodes<<<c->nsm * 2, 256, 0, c->stream>>>(c->ctl, c->stack, c->d_jobnodes);
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->k1, c->stream));
-  CK(cudaMemcpyAsync(c->ctl_host, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(c->h_jobbuf, c->d_jobcnt, sizeof(unsigned long long) * kMaxJobs * kJobCounters,
-                     cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(c->h_jobbuf + kMaxJobs * kJobCounters, c->d_jobnodes, sizeof(unsigned long long) * kMaxJobs,
-                     cudaMemcpyDeviceToHost, c->stream));
+  CK(d2h(c, c->ctl_host, c->ctl, sizeof(Ctl)));
+  CK(d2h(c, c->h_jobbuf, c->d_jobcnt, sizeof(unsigned long long) * kMaxJobs * kJobCounters));
+  CK(d2h(c, c->h_jobbuf + kMaxJobs * kJobCounters, c->d_jobnodes, sizeof(unsigned long long) * kMaxJobs));
   CK(cudaStreamSynchronize(c->stream));
   float ms = 0;
   cudaEventElapsedTime(&ms, c->k0, c->k1);
@@ -1723,15 +1842,13 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
   c->stats.launches += launches;
   c->stats.search_kernel_launches += 1;
   c->stats.epochs += 1;
-  if (c->ctl_host->error) return (c->ctl_host->error & kErrTimeout) ? E13_ERR_TIMEOUT : E13_ERR_OVERFLOW;
   // 3. survivors found in this epoch go to their jobs
   const unsigned long long ns = c->ctl_host->nsurv;
   const unsigned long long avail = std::min<unsigned long long>(ns, (unsigned long long)c->surv_cap);
   if (ns > (unsigned long long)c->surv_cap) s->surv_overflow = true;
   if (avail > s->surv_fetched) {
     std::vector<SurvRec> recs((size_t)(avail - s->surv_fetched));
-    CK(cudaMemcpyAsync(recs.data(), c->surv + s->surv_fetched, sizeof(SurvRec) * recs.size(), cudaMemcpyDeviceToHost,
-                       c->stream));
+    CK(d2h(c, recs.data(), c->surv + s->surv_fetched, sizeof(SurvRec) * recs.size()));
     CK(cudaStreamSynchronize(c->stream));
     for (const SurvRec &r : recs) {
       ServeJob *j = (r.job >= 0 && r.job < kMaxJobs) ? s->slot_job[r.job].get() : nullptr;
@@ -1745,21 +1862,32 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
   // 4. jobs with no node left are done
   const double tdone = e13_serve_clock(s);
   const unsigned long long *cnt = c->h_jobbuf, *nodes = c->h_jobbuf + kMaxJobs * kJobCounters;
+  if (c->ctl_host->error) {
+    // a device wait ran out or an epoch's outputs did not fit: finish_launch
+    // dropped the frontier, so every running job ends with that status and
+    // the partial counts it had; queued jobs run on a cleared control block
+    const int st = (c->ctl_host->error & kErrTimeout) ? E13_ERR_TIMEOUT : E13_ERR_OVERFLOW;
+    for (int k = 0; k < kMaxJobs; ++k) {
+      if (!s->slot_job[k]) continue;
+      ServeJob &j = *s->slot_job[k];
+      fill_result(done[(*ndone)++], j, cnt + k * kJobCounters, st, tdone);
+      s->finished_surv[j.id] = std::move(j.surv);
+      s->slot_job[k].reset();
+    }
+    const int launches_so_far = c->ctl_host->launches;  // pool-slot tags must keep rising
+    memset(c->ctl_host, 0, sizeof(Ctl));
+    c->ctl_host->launches = launches_so_far;
+    CK(h2d(c, c->ctl, c->ctl_host, sizeof(Ctl)));
+    CK(cudaStreamSynchronize(c->stream));
+    s->surv_fetched = 0;
+    s->surv_overflow = false;
+    s->reorder = false;
+    return E13_OK;
+  }
   for (int k = 0; k < kMaxJobs; ++k) {
     if (!s->slot_job[k] || nodes[k] != 0) continue;
     ServeJob &j = *s->slot_job[k];
-    e13_serve_result &r = done[(*ndone)++];
-    memset(&r, 0, sizeof r);
-    r.id = j.id;
-    r.counts.leaves = cnt[k * kJobCounters + 0];
-    r.counts.steps = cnt[k * kJobCounters + 1];
-    for (int h = 0; h <= E13_STAGES; ++h) r.counts.hist[h] = cnt[k * kJobCounters + 2 + h];
-    r.counts.survivors = (uint64_t)j.surv.size();
-    r.nsurv = (int32_t)j.surv.size();
-    r.status = s->surv_overflow ? E13_ERR_SURV_CAP : E13_OK;
-    r.t_submit = j.t_submit;
-    r.t_start = j.t_start;
-    r.t_done = tdone;
+    fill_result(done[(*ndone)++], j, cnt + k * kJobCounters, s->surv_overflow ? E13_ERR_SURV_CAP : E13_OK, tdone);
     s->finished_surv[j.id] = std::move(j.surv);
     s->slot_job[k].reset();
   }
@@ -1767,28 +1895,78 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
   //    from the top: the job with the most live nodes at the bottom, the one
   //    with the fewest on top (nearly finished jobs finish first); on a tie the
   //    job started later goes higher.  Only when every node is accounted for.
-  {
-    int order[kMaxJobs], n = 0;
-    for (int k = 0; k < kMaxJobs; ++k)
-      if (s->slot_job[k] && nodes[k] > 0) order[n++] = k;
-    if (n > 1) {
-      std::sort(order, order + n, [&](int a, int b) {
-        if (nodes[a] != nodes[b]) return nodes[a] > nodes[b];
-        return s->slot_job[a]->t_start < s->slot_job[b]->t_start;
-      });
-      unsigned long long off = 0;
-      memset(s->fill, 0, sizeof s->fill);
-      for (int i = 0; i < n; ++i) {
-        s->fill[order[i]] = off;
-        off += nodes[order[i]];
+  int order[kMaxJobs], n = 0;
+  unsigned long long accounted = 0;
+  for (int k = 0; k < kMaxJobs; ++k)
+    if (s->slot_job[k] && nodes[k] > 0) {
+      order[n++] = k;
+      accounted += nodes[k];
+    }
+  std::sort(order, order + n, [&](int a, int b) {
+    if (nodes[a] != nodes[b]) return nodes[a] > nodes[b];
+    return s->slot_job[a]->t_start < s->slot_job[b]->t_start;
+  });
+  const bool complete = accounted == (unsigned long long)c->ctl_host->top;
+  // 6. too little room for the next epoch's outputs: swap jobs out, the one
+  //    with the most live nodes first, until the rest fits.  A swapped-out
+  //    job's frontier nodes and counters go to host memory and it goes back to
+  //    the head of the queue; re-admitted, it goes on where it stopped (its
+  //    counts stay exact).  A job that does not fit alone fails with
+  //    E13_ERR_OVERFLOW.
+  const long long cur_top = c->ctl_host->top;
+  if (complete && n > 0 && cur_top + s->out_nodes > s->cap) {
+    int first = 0;  // order[0..first) leave the frontier, order[first..n) stay
+    long long after = cur_top;
+    while (n - first > 1 && after + s->out_nodes > s->cap) after -= (long long)nodes[order[first++]];
+    if (after + s->out_nodes > s->cap) {
+      // one job left and it alone does not fit: it fails, its nodes are dropped
+      const int k = order[first++];
+      ServeJob &j = *s->slot_job[k];
+      fill_result(done[(*ndone)++], j, cnt + k * kJobCounters, E13_ERR_OVERFLOW, tdone);
+      s->finished_surv[j.id] = std::move(j.surv);
+      s->slot_job[k].reset();
+      after -= (long long)nodes[k];
+    }
+    // bottom to top: the jobs that stay in the usual order, then the ones
+    // leaving, which are then copied out from above the new top
+    int lay[kMaxJobs], m = 0;
+    for (int i = first; i < n; ++i) lay[m++] = order[i];
+    for (int i = first - 1; i >= 0; --i) lay[m++] = order[i];
+    int rc;
+    if ((rc = regroup(s, lay, m, nodes))) return rc;
+    long long pos = after;
+    for (int i = first - 1; i >= 0; --i) {
+      const int k = order[i];
+      if (s->slot_job[k]) {
+        std::unique_ptr<ServeJob> j = std::move(s->slot_job[k]);
+        j->saved.resize((size_t)nodes[k]);
+        CK(d2h(c, j->saved.data(), c->stack + pos, sizeof(Node) * (size_t)nodes[k]));
+        memcpy(j->saved_cnt, cnt + k * kJobCounters, sizeof j->saved_cnt);
+        j->swapped = true;
+        j->reserve = std::max<long long>(j->reserve, 2 * (long long)nodes[k]);
+        j->slot = -1;
+        s->queue.push_front(std::move(j));
+        ++s->evictions;
       }
-      s->reorder = off == (unsigned long long)c->ctl_host->top;
+      pos += (long long)nodes[k];
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    if ((rc = set_top(s, after))) return rc;
+    n = 0;  // the frontier is in order already
+  }
+  if (n > 1 && complete) s->reorder = true;
+  if (s->reorder) {
+    unsigned long long off = 0;
+    memset(s->fill, 0, sizeof s->fill);
+    for (int i = 0; i < n; ++i) {
+      s->fill[order[i]] = off;
+      off += nodes[order[i]];
     }
   }
-  // 6. idle: start the survivor buffer over
+  // 7. idle: start the survivor buffer over
   if (e13_serve_pending(s) == 0) {
     unsigned long long zero = 0;
-    CK(cudaMemcpyAsync(&c->ctl->nsurv, &zero, sizeof zero, cudaMemcpyHostToDevice, c->stream));
+    CK(h2d(c, &c->ctl->nsurv, &zero, sizeof zero));
     CK(cudaStreamSynchronize(c->stream));
     s->surv_fetched = 0;
     s->surv_overflow = false;
@@ -1809,9 +1987,10 @@ extern "C" int e13_serve_survivors(e13_serve *s, int64_t id, e13_survivor *out, 
   return rc;
 }
 
-extern "C" int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs) {
+extern "C" int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs, int64_t *swapped_out) {
   if (!s) return E13_ERR_ARG;
   if (device_ms) *device_ms = s->device_ms;
   if (epochs) *epochs = s->epochs;
+  if (swapped_out) *swapped_out = s->evictions;
   return E13_OK;
 }

@@ -80,7 +80,7 @@ class Stats(ctypes.Structure):
                 ("peak_nodes", ctypes.c_int64), ("search_kernel_launches", ctypes.c_int64),
                 ("search_kernel_ms", ctypes.c_double), ("lane_occupancy", ctypes.c_double),
                 ("warp_rounds", ctypes.c_int64), ("donations", ctypes.c_int64), ("pool_claims", ctypes.c_int64),
-                ("idle_polls", ctypes.c_int64)]
+                ("idle_polls", ctypes.c_int64), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64)]
 
 
 class ServeResult(ctypes.Structure):
@@ -135,6 +135,8 @@ def lib():
         L.e13_format_summary.argtypes = [P(Job), P(Counts), ctypes.c_double, ctypes.c_char_p, ctypes.c_size_t]
         L.e13_default_tuning.argtypes = [P(Tuning)]
         L.e13_default_tuning.restype = None
+        L.e13_resolve_tuning.argtypes = [P(Tuning), I, P(Tuning)]
+        L.e13_selftest_pool_wait.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         L.e13_ctx_create.argtypes = [I, P(ctypes.c_void_p)]
         L.e13_ctx_destroy.argtypes = [ctypes.c_void_p]
         L.e13_ctx_destroy.restype = None
@@ -158,7 +160,7 @@ def lib():
         L.e13_serve_pending.argtypes = [ctypes.c_void_p]
         L.e13_serve_pending.restype = ctypes.c_int64
         L.e13_serve_survivors.argtypes = [ctypes.c_void_p, ctypes.c_int64, P(Survivor), I, P(I)]
-        L.e13_serve_stats.argtypes = [ctypes.c_void_p, P(ctypes.c_double), P(ctypes.c_int64)]
+        L.e13_serve_stats.argtypes = [ctypes.c_void_p, P(ctypes.c_double), P(ctypes.c_int64), P(ctypes.c_int64)]
         L.e13_run_full.argtypes = [ctypes.c_void_p, P(ctypes.c_int32), I, I, P(ctypes.c_int64)]
         L.e13_check.argtypes = [ctypes.c_void_p, P(CheckIn), I, I, I, P(CheckOut)]
         L.e13_check_noalloc.argtypes = [I, P(CheckIn), I, I, I, P(CheckOut)]
@@ -176,7 +178,8 @@ EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine
             "e13_search", "e13_search_shard", "e13_search_resumable", "e13_estimate", "e13_last_stats", "e13_run_full", "e13_check", "e13_parse_survivor_line",
             "e13_format_recheck", "e13_format_deep", "e13_check_crafted", "e13_raw_run", "e13_autotune", "e13_check_noalloc",
             "e13_serve_create", "e13_serve_destroy", "e13_serve_clock", "e13_serve_submit", "e13_serve_step",
-            "e13_serve_pending", "e13_serve_survivors", "e13_serve_stats"]
+            "e13_serve_pending", "e13_serve_survivors", "e13_serve_stats", "e13_resolve_tuning",
+            "e13_selftest_pool_wait"]
 
 
 def keys():
@@ -227,6 +230,14 @@ def tuning(**kw) -> Tuning:
     return t
 
 
+def resolve_tuning(tune: Tuning | None, serve: bool = False):
+    """(status, Tuning): the tuning a search or serve session would run with
+    (e13_resolve_tuning); status E13_ERR_ARG for a field out of range."""
+    out = Tuning()
+    r = lib().e13_resolve_tuning(ctypes.byref(tune) if tune else None, 1 if serve else 0, ctypes.byref(out))
+    return r, out
+
+
 class Context:
     """A device context (one CUDA device, one stream, reusable buffers)."""
 
@@ -256,6 +267,11 @@ class Context:
         if r and r != -7:
             raise E13Error(r, "e13_search")
         return counts, [surv[i] for i in range(min(ns.value, surv_cap))]
+
+    def selftest_pool_wait(self, wait_us: int) -> int:
+        """Status of e13_selftest_pool_wait: E13_ERR_TIMEOUT (-10) when the
+        persistent kernel's bounded pool wait runs out as it should."""
+        return lib().e13_selftest_pool_wait(self.h, wait_us)
 
     def search_shard(self, job: Job, shard: int, nshards: int, tune: Tuning | None = None, surv_cap: int = 1 << 16):
         """Shard `shard` of `nshards` of the search for `job` (e13_search_shard)."""
@@ -340,15 +356,18 @@ class Context:
             raise E13Error(r, "e13_run_full")
         return [list(out[7 * i: 7 * i + 7]) for i in range(n)]
 
-    def raw_run(self, n, nq=13, max_steps=1 << 18, seed=0, codes: bytes | None = None, want_out=True):
-        """Raw-simulator set; returns (per-machine [steps, status, head, ones] or None, total steps)."""
+    def raw_run(self, n, nq=13, max_steps=1 << 18, seed=0, codes: bytes | None = None, want_out=True,
+                as_array=False):
+        """Raw-simulator set; returns (per-machine [steps, status, head, ones] or None, total steps).
+        as_array: the rows as one flat ctypes int64 array (4 per machine) instead of lists."""
         out = (ctypes.c_int64 * (4 * n))() if want_out else None
         tot = ctypes.c_uint64()
         r = lib().e13_raw_run(self.h, codes, seed, n, nq, max_steps, out, ctypes.byref(tot))
         if r:
             raise E13Error(r, "e13_raw_run")
-        rows = [list(out[4 * i: 4 * i + 4]) for i in range(n)] if want_out else None
-        return rows, tot.value
+        if as_array or not want_out:
+            return out, tot.value
+        return [list(out[4 * i: 4 * i + 4]) for i in range(n)], tot.value
 
     def check(self, ins, nmax, mode=0):
         n = len(ins)
@@ -451,10 +470,17 @@ class Server:
         return [out[i] for i in range(min(n.value, cap))]
 
     def stats(self):
+        """(device ms of all epochs, epochs)."""
         ms = ctypes.c_double()
         ep = ctypes.c_int64()
-        lib().e13_serve_stats(self.h, ctypes.byref(ms), ctypes.byref(ep))
+        lib().e13_serve_stats(self.h, ctypes.byref(ms), ctypes.byref(ep), None)
         return ms.value, ep.value
+
+    def swapped_out(self) -> int:
+        """Times a job was swapped out to host memory to make room."""
+        n = ctypes.c_int64()
+        lib().e13_serve_stats(self.h, None, None, ctypes.byref(n))
+        return n.value
 
     def run_all(self, jobs, arrivals=None):
         """Submits jobs (with optional arrival times) and steps until all are

@@ -83,10 +83,12 @@ enum {
   E13_KERNEL_PERSISTENT = 1  /* per-warp DFS with in-kernel work donation, graph-captured epochs */
 };
 
-/* Tunables of the device search (0 = library default; see e13_default_tuning). */
+/* Tunables of the device search.  kernel and run_skip are taken as given; in
+   every other field 0 means the library default (e13_default_tuning) and a
+   negative value is an error.  e13_resolve_tuning states the valid ranges. */
 typedef struct e13_tuning {
   int32_t kernel;            /* E13_KERNEL_* */
-  int32_t block;             /* lanes (threads) per CTA: 128..896, multiple of 32 */
+  int32_t block;             /* lanes (threads) per CTA: 64..768, multiple of 32 */
   int32_t slice;             /* steps per round between warp-level refills */
   int32_t warp_stack;        /* nodes in each warp's private DFS stack (persistent) */
   int32_t step_cap;          /* plain kernel: steps per work item before it is requeued */
@@ -112,6 +114,8 @@ typedef struct e13_stats {
   int64_t donations;         /* persistent: stack nodes donated to the pool */
   int64_t pool_claims;       /* persistent: pool nodes taken by warps without work */
   int64_t idle_polls;        /* persistent: polls by warps waiting for work */
+  int64_t h2d_bytes;         /* host-to-device bytes the call copied (roots, control words, checkpoints) */
+  int64_t d2h_bytes;         /* device-to-host bytes the call copied (control words, counters, survivors) */
 } e13_stats;
 
 typedef struct e13_ctx e13_ctx;
@@ -151,6 +155,18 @@ int e13_format_summary(const e13_job *job, const e13_counts *c, double wall_s, c
 
 /* Fills t with the library defaults for this device. */
 void e13_default_tuning(e13_tuning *t);
+
+/* The tuning a search (serve = 0) or a serve session (serve = 1) runs with:
+   the defaults, overridden by the nonzero fields of `in` (NULL: defaults; a
+   serve session defaults to 10 ms epochs and always uses the persistent
+   kernel).  Returns E13_ERR_ARG, and leaves *out alone, unless every field is
+   in range: kernel 0..1, run_skip 0..1, block 64..768 and a multiple of 32,
+   slice 1..4096, warp_stack 1..4096, epoch_us 1..6e7, epochs_per_graph 1..64,
+   pool_low_pct 1..100, and step_cap, batch, stack_nodes >= 0.  Every
+   entry point that takes a tuning applies this check first.  No counterpart
+   in the reference, whose only knobs are E13_SPLIT (src/e13search.c:47-49)
+   and E13_SLICE (src/e13gpu.py:342-346). */
+int e13_resolve_tuning(const e13_tuning *in, int serve, e13_tuning *out);
 
 /* ---- device path ---- */
 
@@ -228,7 +244,14 @@ typedef struct e13_estimate_out {
    seed = E13_SEED), so every probe's counts depend only on (seed, p).
    per_probe (may be NULL): 4 doubles per probe, leaves, nodes, steps,
    survivors.  No counterpart of the per-probe layout in the reference, which
-   sums per thread. */
+   sums per thread.  The reference hands probes to threads dynamically, so its
+   printed numbers depend on scheduling; the numbers here are a different
+   sample of the same estimator and match the reference probe for probe only
+   (each probe's counts equal the oracle's restatement of probe() on the same
+   stream), not line for line.  probes is at most E13_ESTIMATE_MAX_PROBES
+   (2^20, the stride between the stream starts of seed and seed + 1), else
+   E13_ERR_ARG. */
+#define E13_ESTIMATE_MAX_PROBES (1LL << 20)
 int e13_estimate(e13_ctx *ctx, const e13_job *job, int64_t probes, uint64_t seed, e13_estimate_out *out,
                  double *per_probe);
 
@@ -237,20 +260,39 @@ int e13_estimate(e13_ctx *ctx, const e13_job *job, int64_t probes, uint64_t seed
 /* Continuous batching of search jobs (no counterpart in the reference, which
    runs one search per process).  Up to 16 jobs share the persistent kernel:
    every node carries its job's slot, and each job has its own counters and
-   survivors.  A job is admitted when a slot is free, its submit time has
-   passed and the frontier stack has room for every running job's reservation
-   (reserve_nodes, 0 = 64 Ki nodes) plus its own; the serve stack holds
-   tuning->stack_nodes nodes (0 = 16 Mi nodes, 5 GB), and a second buffer of
-   the same size lets the frontier be regrouped between epochs, the job with
-   the fewest live nodes on top.  e13_serve_step admits, runs one epoch
-   (tuning->epoch_us, default 10 ms) and returns the jobs that finished in it:
-   a job is finished when none of its nodes is left on the frontier.  Each
-   job's counts equal those of e13_search on that job alone.
-   A context runs one serve session at a time and no e13_search meanwhile. */
+   survivors.
+
+   Admission is by the frontier memory a job needs.  e13_serve_submit sizes
+   each job with the Knuth estimator (e13_estimate, 64 probes, seed 0): the
+   frontier of a search never holds more machines than its tree has nodes and
+   leaves, so a job whose estimated tree is below one epoch's dump of every
+   warp reserves twice its estimate (at least 64 nodes), and a larger job
+   reserves that dump bound.  reserve_nodes > 0 replaces the estimate by a
+   fixed reservation per job.  First come, first served, a queued job is
+   admitted when a slot is free, its submit time has passed and the frontier
+   has room for every running job's reservation plus its own; a job alone is
+   always admitted.  The serve stack holds tuning->stack_nodes nodes (0 = 16 Mi
+   nodes, 5 GB), and a second buffer of the same size lets the frontier be
+   regrouped between epochs, the job with the fewest live nodes on top.
+
+   Estimates can be wrong.  When, after an epoch, the frontier leaves less
+   room than the next epoch may need, jobs are swapped out, the one with the
+   most live nodes first: its nodes and counters go to host memory and it goes
+   back to the head of the queue, reserving twice the nodes it had; re-admitted,
+   it goes on where it stopped, so its counts stay exact.  A job that does not
+   fit even alone ends with status E13_ERR_OVERFLOW, and so does every running
+   job when a device wait runs out (E13_ERR_TIMEOUT); the session goes on.
+
+   e13_serve_step admits, runs one epoch (tuning->epoch_us, default 10 ms)
+   and returns the jobs that finished in it: a job is finished when none of its
+   nodes is left on the frontier.  Each job's counts equal those of e13_search
+   on that job alone.  A context runs one serve session at a time and no
+   e13_search meanwhile. */
 typedef struct e13_serve e13_serve;
 typedef struct e13_serve_result {
   int64_t id;
-  int32_t status;            /* E13_OK, or E13_ERR_SURV_CAP if survivor records were lost */
+  int32_t status;            /* E13_OK; E13_ERR_SURV_CAP if survivor records were lost; E13_ERR_OVERFLOW /
+                                E13_ERR_TIMEOUT if the job was cut short (counts then partial) */
   int32_t nsurv;             /* survivor records kept for e13_serve_survivors */
   e13_counts counts;
   double t_submit, t_start, t_done; /* seconds on the serve clock */
@@ -260,7 +302,8 @@ int e13_serve_create(e13_ctx *ctx, const e13_tuning *tuning, int64_t reserve_nod
 void e13_serve_destroy(e13_serve *s);
 /* Seconds since e13_serve_create. */
 double e13_serve_clock(const e13_serve *s);
-/* Queues a job; t_submit < 0 means now (serve clock). */
+/* Queues a job; t_submit < 0 means now (serve clock).  Unless the session has
+   a fixed reservation, runs the job's size estimate on the device first. */
 int e13_serve_submit(e13_serve *s, const e13_job *job, int64_t id, double t_submit);
 /* One admission + epoch + completion pass; done needs room for 16 results. */
 int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int *ndone);
@@ -268,8 +311,9 @@ int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int *ndone);
 int64_t e13_serve_pending(const e13_serve *s);
 /* Survivors of a finished job (once; *n = all it found). */
 int e13_serve_survivors(e13_serve *s, int64_t id, e13_survivor *out, int cap, int *n);
-/* CUDA-event time of all epochs and their number. */
-int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs);
+/* CUDA-event time of all epochs, their number, and how many times a job was
+   swapped out to host memory to make room (each pointer may be NULL). */
+int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs, int64_t *swapped_out);
 
 /* Autotuner (no counterpart in the reference, which has one fixed GPU
    launch shape): coordinate descent over block size (lanes per CTA), slice
@@ -280,6 +324,16 @@ int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs);
    reproduce the same counts, else E13_ERR_CUDA.  start may be NULL
    (defaults); *best_ms (may be NULL) is the best device time. */
 int e13_autotune(e13_ctx *ctx, const e13_job *job, const e13_tuning *start, e13_tuning *best, double *best_ms);
+
+/* Self-test of the persistent kernel's one device-side wait, for a caller
+   (or a test) that wants to see a device wait run out without a hang: runs
+   one epoch in which a warp claims a donation-pool slot whose data never
+   arrives.  The warp waits wait_us (1 .. 1e6) for it, flags the timeout and
+   the epoch ends.  Returns E13_ERR_TIMEOUT when the bounded wait works as it
+   should; the context stays usable (the next search starts from a clean
+   control block).  No counterpart in the reference, which has no device-side
+   waits. */
+int e13_selftest_pool_wait(e13_ctx *ctx, int32_t wait_us);
 
 /* Statistics of the last e13_search on this context. */
 int e13_last_stats(const e13_ctx *ctx, e13_stats *out);
@@ -359,11 +413,17 @@ int e13_check(e13_ctx *ctx, const e13_check_in *in, int n, int nmax, int mode, e
    outputs of at most E13_CHECK_NOALLOC_MAX machines live in fixed device
    arrays compiled into the library (about 16 MB, held by every GPU that loads
    it until the process exits); n above that returns E13_ERR_NOALLOC_SIZE.
-   in/out are host arrays of n entries, as for e13_check; the call is
-   synchronous on `device`.  Its first call on a device looks up the arrays'
-   device addresses (cudaGetSymbolAddress), so make that first call before any
-   stream capture.  All calls share the arrays: calls that overlap on the same
-   GPU (other host threads) race and must be serialised by the caller. */
+   in/out are host arrays of n entries, as for e13_check.  The work runs on a
+   non-blocking stream of this entry point's own, one per device, and the call
+   returns after synchronising that stream only (no device-wide wait, so a
+   kernel the caller runs on another stream is not waited for).  Its first call
+   on a device, with that device current, looks up the arrays' device addresses
+   (cudaGetSymbolAddress) and creates that stream, once per device even when
+   several threads make the first call together; make that first call before
+   any stream capture.  All calls share the arrays and keep the last call's
+   contents (each call clears what must start at zero): calls that overlap on
+   the same GPU (other host threads) race and must be serialised by the
+   caller. */
 #define E13_CHECK_NOALLOC_MAX 16
 int e13_check_noalloc(int device, const e13_check_in *in, int n, int nmax, int mode, e13_check_out *out);
 

@@ -45,7 +45,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 ARGS = [a for a in sys.argv[1:] if a not in ("estimates", "checks")]
-REF = ARGS[0] if ARGS else "/root/reference"
+REF = ARGS[0] if ARGS else os.environ.get("E13_REF", "/root/reference")
 RES = os.path.join(REF, "results")
 REFBIN = os.path.join(REPO, "oracle", "_ref", "e13search")
 

@@ -167,6 +167,30 @@ def test_raw_simulator_vs_oracle():
     assert got2 == exp
 
 
+def test_raw_simulator_full_set_vs_reference_run_loop():
+    """The whole raw set on the device (1e6 random 13-state machines from seed
+    0, <= 2^18 steps each): its per-machine results aggregate exactly to
+    tests/golden/raw_1e6.json, which make_raw_golden.py made by running the
+    same tables through the reference's own run() (src/e13search.c:134-177)
+    with the filter switched off -- total steps, machines by status, final
+    heads by status, and an order-dependent checksum of every machine's row."""
+    import json
+    import os
+    import sys
+
+    import numpy as np
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, gold)
+    import make_raw_golden as G
+    g = json.load(open(os.path.join(gold, "raw_1e6.json")))
+    out, tot = ctx().raw_run(g["machines"], nq=g["nq"], max_steps=g["max_steps"], seed=g["seed"], as_array=True)
+    rows = np.ctypeslib.as_array(out).reshape(-1, 4)
+    agg = G.aggregates(rows)
+    assert tot == g["total_steps"]
+    for k in ("machines", "total_steps", "by_status", "head_hist_by_status", "sum_head", "sum_ones", "checksum"):
+        assert agg[k] == g[k], k
+
+
 def test_run_full_matches_oracle_random_tables():
     """Whole-table runs (with the filter) of random 13-state tables against
     the oracle."""

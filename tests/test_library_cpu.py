@@ -250,3 +250,28 @@ def test_e13gpu_script_refuses_like_the_reference():
     assert p.returncode == 1 and "named by a fixed cell" in p.stderr
     p = _e13gpu([machine, "13", "0", "13", "A0", "A1"])
     assert p.returncode == 1 and ("start state" in p.stderr or "named by a fixed cell" in p.stderr)
+
+
+def test_tuning_ranges_are_checked():
+    """e13_resolve_tuning (applied by every entry point that takes a tuning):
+    zero fields take the defaults, a serve session defaults to 10 ms epochs on
+    the persistent kernel, and each field out of range is E13_ERR_ARG --
+    including a negative epoch bound (it would make one launch run a whole
+    search, so checkpoints and stop files never fire) and a negative or zero
+    graph length (an empty graph would never move the frontier)."""
+    r, t = E.resolve_tuning(None)
+    d = E.tuning()
+    assert r == 0 and (t.block, t.slice, t.warp_stack, t.epoch_us, t.epochs_per_graph, t.pool_low_pct) == \
+        (d.block, d.slice, d.warp_stack, d.epoch_us, d.epochs_per_graph, d.pool_low_pct)
+    r, t = E.resolve_tuning(E.tuning(kernel=E.KERNEL_PLAIN, epoch_us=0), serve=True)
+    assert r == 0 and t.kernel == E.KERNEL_PERSISTENT and t.epoch_us == 10000
+    r, t = E.resolve_tuning(E.tuning(slice=9, block=256))
+    assert r == 0 and t.slice == 9 and t.block == 256
+    bad = [dict(epoch_us=-1), dict(epochs_per_graph=-1), dict(pool_low_pct=-5), dict(pool_low_pct=101),
+           dict(block=48), dict(block=800), dict(block=100), dict(slice=-1), dict(slice=5000),
+           dict(warp_stack=-2), dict(warp_stack=5000), dict(epochs_per_graph=65), dict(epoch_us=60_000_001),
+           dict(step_cap=-1), dict(batch=-1), dict(stack_nodes=-1), dict(kernel=2), dict(run_skip=2)]
+    for kw in bad:
+        for serve in (False, True):
+            r, _ = E.resolve_tuning(E.tuning(**kw), serve=serve)
+            assert r == -1, (kw, serve)

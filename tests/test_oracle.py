@@ -192,6 +192,42 @@ def test_raw_run_small_known_cases():
     assert O.raw_run(codes, 1, nq=13)[0] == [63, 1, -64, 0]
 
 
+REF_RAW = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "ref_raw")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_RAW), reason="oracle/_ref/ref_raw not built (no reference checkout)")
+def test_raw_run_equals_reference_run_loop():
+    """The raw-simulator restatement against the reference's own step loop:
+    oracle/_ref/ref_raw runs run() of src/e13search.c with the filter switched
+    off from outside.  Per machine (steps, status, final head, ones), on 20,000
+    machines of the set and on 2,000 machines of an 8-state set with a short cap."""
+    import numpy as np
+    for seed, m0, n, nq, cap in ((0, 0, 20000, 13, 1 << 18), (5, 777, 2000, 8, 5000)):
+        p = subprocess.run([REF_RAW, str(seed), str(m0), str(n), str(nq), str(cap)], capture_output=True, check=True)
+        ref = np.frombuffer(p.stdout, dtype=np.int64).reshape(-1, 4)
+        codes = O.raw_tables(seed, m0 + n, nq)[m0 * 2 * nq:]
+        got = np.array(O.raw_run(codes, n, nq=nq, max_steps=cap), dtype=np.int64).reshape(-1, 4)
+        assert (got == ref).all()
+
+
+def test_raw_golden_fixture_matches_its_first_machines():
+    """raw_1e6.json (made by tests/golden/make_raw_golden.py from the
+    reference's run()) is consistent with the oracle: the histogram counts add
+    up, and the oracle's first 2,000 machines have the checksum the generator's
+    function gives them."""
+    import sys
+    sys.path.insert(0, GOLD)
+    import make_raw_golden as G
+    g = json.load(open(os.path.join(GOLD, "raw_1e6.json")))
+    assert g["machines"] == 1000000 and sum(g["by_status"].values()) == 1000000
+    for s, h in g["head_hist_by_status"].items():
+        assert sum(h.values()) == g["by_status"][s]
+    codes = O.raw_tables(0, 2000)
+    out = O.raw_run(codes, 2000)
+    agg = G.aggregates(out)
+    assert agg["machines"] == 2000 and agg["total_steps"] == sum(r[0] for r in out)
+
+
 def _estimate_job(case):
     args = case["args"]
     X, fmax, lo, hi = int(args[3]), int(args[4]), int(args[5]), int(args[6])
