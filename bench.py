@@ -29,9 +29,10 @@ Every measured search is checked against the reference's logs (leaves,
 survivors, deaths per stage, steps where logged, sorted survivor lines).
 
 --impl reference runs the reference CPU program instead (the reference arm).
-Under torchrun (N > 1) rank r runs every N-th X starting at r (the search
-splits into independent per-X jobs; e13shard.py sums the totals and takes the
-maximum of the times over ranks).
+Under torchrun (N > 1) every rank runs its share of every job: each job's
+frontier is expanded and dealt out by content (e13_serve_submit_shard), so the
+ranks carry equal work whatever the jobs' sizes; e13shard.py sums the counts
+and takes the maximum of the times over ranks.
 """
 from __future__ import annotations
 
@@ -95,12 +96,13 @@ def parity_of(w, per_job, lines):
     ok = {"leaves": True, "survivors": True, "hist": True, "steps": True}
     steps_checked = 0
     for X, c in per_job.items():
+        c = c if isinstance(c, dict) else c.as_dict()
         e = exp[X]
-        ok["leaves"] &= c.leaves == e["leaves"]
-        ok["survivors"] &= c.survivors == e["survivors"]
-        ok["hist"] &= list(c.hist) == e["hist"]
+        ok["leaves"] &= c["leaves"] == e["leaves"]
+        ok["survivors"] &= c["survivors"] == e["survivors"]
+        ok["hist"] &= list(c["hist"]) == e["hist"]
         if e["steps"] is not None:
-            ok["steps"] &= c.steps == e["steps"]
+            ok["steps"] &= c["steps"] == e["steps"]
             steps_checked += 1
     ok["survivor_lines"] = sorted(lines) == golden_lines(g) if g.get("survivors_file") else (len(lines) == 0)
     ok["jobs_with_logged_steps"] = steps_checked
@@ -313,13 +315,22 @@ def roofline(steps, seconds, sm_mhz, nsm):
     return {"bound": "int-issue", "achieved": ach, "peak": peak, "unit": "Gop/s", "frac": ach / peak}
 
 
-def run_concurrent(E, ctx, jobs, epoch_us=200000, stack_nodes=0):
-    """All jobs in one serve session of the persistent kernel.  Returns
-    ({X: Counts}, survivor lines, device ms, launches, h2d, d2h, wall s)."""
+def serve_tuning(E, tuned, stack_nodes=0):
+    """The headline's serve session: the autotuned launch shape, 200 ms epochs."""
+    t = E.tuning(epoch_us=200000, stack_nodes=stack_nodes)
+    if tuned is not None:
+        t.block, t.slice, t.warp_stack, t.pool_low_pct = tuned.block, tuned.slice, tuned.warp_stack, tuned.pool_low_pct
+    return t
+
+
+def run_concurrent(E, ctx, jobs, tune, shard=0, nshards=1):
+    """All jobs (with nshards > 1: this rank's share of each) in one serve
+    session of the persistent kernel.  Returns ({X: Counts}, survivor lines,
+    device ms, launches, h2d, d2h, wall s)."""
     per, lines = {}, []
     t0 = time.perf_counter()
-    with E.Server(ctx, E.tuning(epoch_us=epoch_us, stack_nodes=stack_nodes)) as srv:
-        got = srv.run_all([j for _, j in jobs])
+    with E.Server(ctx, tune) as srv:
+        got = srv.run_all([j for _, j in jobs], shard=shard, nshards=nshards)
         ms, _ = srv.stats()
     wall = time.perf_counter() - t0
     st = ctx.stats()
@@ -330,11 +341,14 @@ def run_concurrent(E, ctx, jobs, epoch_us=200000, stack_nodes=0):
     return per, lines, ms, st.launches, st.h2d_bytes, st.d2h_bytes, wall
 
 
-def run_sequential(E, ctx, jobs, kernel):
+def run_sequential(E, ctx, jobs, kernel, tuned=None):
     """Each job alone with e13_search on one kernel, one after another."""
     per, lines, ms, launches = {}, [], 0.0, 0
+    t = E.tuning(kernel=kernel)
+    if tuned is not None:
+        t.block, t.slice, t.warp_stack, t.pool_low_pct = tuned.block, tuned.slice, tuned.warp_stack, tuned.pool_low_pct
     for X, job in jobs:
-        c, surv = ctx.search(job, E.tuning(kernel=kernel))
+        c, surv = ctx.search(job, t)
         st = ctx.stats()
         per[X] = c
         lines += [E.survivor_line(job, s) for s in surv]
@@ -343,9 +357,11 @@ def run_sequential(E, ctx, jobs, kernel):
     return per, lines, ms, launches
 
 
-def kernel_comparison(E, torch, ctx, flush, local, nsm):
+def kernel_comparison(E, torch, ctx, flush, local, nsm, tuned):
     """Persistent vs plain on the same searches, both run the same way: each
-    job of the workload alone, one after another."""
+    job of the workload alone, one after another, with the same autotuned
+    block size and slice (warp stack and pool threshold exist only in the
+    persistent kernel)."""
     out = {}
     for name in ("local_edits_f4", "counter_sym"):
         w = WORKLOADS[name]
@@ -356,7 +372,7 @@ def kernel_comparison(E, torch, ctx, flush, local, nsm):
             torch.cuda.synchronize()
             sampler = ClockSampler(local)
             with sampler:
-                per, lines, ms, launches = run_sequential(E, ctx, jobs, k)
+                per, lines, ms, launches = run_sequential(E, ctx, jobs, k, tuned)
             clocks = sampler.summary()
             steps = sum(c.steps for c in per.values())
             leaves = sum(c.leaves for c in per.values())
@@ -435,6 +451,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="headline only (no kernel comparison, serving, raw set)")
     ap.add_argument("--stack-nodes", type=int, default=0, help="frontier capacity of the serve session (0: default)")
+    ap.add_argument("--no-autotune", action="store_true", help="library default tuning instead of the autotuner's")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     ws, rank, local, pg = dist_setup()
@@ -450,13 +467,25 @@ def main():
         return serving_bench(args, w, ws, rank, local, pg)
     import e13shard as S
 
-    jobs = make_jobs(E, w, S.share(w["X"], rank, ws))
+    jobs = make_jobs(E, w)  # every rank takes a share of every job (e13_serve_submit_shard)
     ctx = E.Context(local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     nsm = torch.cuda.get_device_properties(local).multi_processor_count
 
+    tuned, tuning_cfg = None, {"autotuned": False}
+    if not args.no_autotune:
+        # the autotuner times candidates on 1/8 of this rank's largest job (by the reference's log)
+        exp = {e["X"]: e["leaves"] for e in golden(w["golden"])["expect"]}
+        X, pj = max(jobs, key=lambda xj: exp.get(xj[0], 0))
+        t0 = time.perf_counter()
+        tuned, pms = ctx.autotune(pj, proxy_shards=8)
+        tuning_cfg = {"autotuned": True, "proxy": f"shard 0 of 8 of X={X}", "proxy_ms": pms,
+                      "autotune_wall_s": time.perf_counter() - t0, "block": tuned.block, "slice": tuned.slice,
+                      "warp_stack": tuned.warp_stack, "pool_low_pct": tuned.pool_low_pct}
+    tune = serve_tuning(E, tuned, args.stack_nodes)
+
     for _ in range(args.warmup):
-        run_concurrent(E, ctx, jobs, stack_nodes=args.stack_nodes)
+        run_concurrent(E, ctx, jobs, tune, rank, ws)
     torch.cuda.synchronize()
     tot = dict(steps=0, leaves=0, dev_ms=0.0, wall=0.0, launches=0, h2d=0, d2h=0)
     per_all, lines_all = {}, []
@@ -467,7 +496,7 @@ def main():
         for _ in range(args.steps):
             flush.zero_()  # evict L2 (126 MB) between timed steps
             torch.cuda.synchronize()
-            per, lines, ms, nl, h2d, d2h, wall = run_concurrent(E, ctx, jobs, stack_nodes=args.stack_nodes)
+            per, lines, ms, nl, h2d, d2h, wall = run_concurrent(E, ctx, jobs, tune, rank, ws)
             torch.cuda.synchronize()
             tot["wall"] += wall
             tot["steps"] += sum(c.steps for c in per.values())
@@ -480,12 +509,15 @@ def main():
     if pg:
         pg.barrier()
     clocks = sampler.summary()
-    par = parity_of(w, per_all, lines_all) if ws == 1 else None
     if pg:
         sums, maxes = S.reduce_totals(pg, {k: tot[k] for k in ("steps", "leaves", "launches", "h2d", "d2h")},
                                       {k: tot[k] for k in ("dev_ms", "wall")}, device=f"cuda:{local}")
         tot.update(sums)
         tot.update(maxes)
+        # the last step's per-job counts summed over the shards, and all survivor lines
+        per_all = S.sum_counts(pg, {X: c.as_dict() for X, c in per_all.items()}, device=f"cuda:{local}")
+        lines_all = S.gather_lines(pg, lines_all)
+    par = parity_of(w, per_all, lines_all)
     dev_s = tot["dev_ms"] / 1000.0
     value = tot["steps"] / dev_s
     sm_mhz = clocks["sm_mhz"] or 1965.0
@@ -499,15 +531,15 @@ def main():
             "leaves_per_s": tot["leaves"] / dev_s, "parity": par,
             "config": {"workload": f"{args.workload}: {w['desc']}", "kernel": "persistent",
                        "jobs": f"{len(jobs)} job(s) concurrent in one serve session",
-                       "l2": "flushed between steps (256 MiB write)",
-                       "parallelism": f"X sharded over {ws} rank(s)"},
+                       "l2": "flushed between steps (256 MiB write)", "tuning": tuning_cfg,
+                       "parallelism": f"every job's subtrees dealt over {ws} rank(s)" if ws > 1 else "1 GPU"},
             "roofline": rl,
             "e2e": {"value": tot["steps"] / tot["wall"], "unit": "steps/s",
                     "h2d_bytes_per_step": tot["h2d"] // args.steps, "d2h_bytes_per_step": tot["d2h"] // args.steps,
                     "note": "host clock around the C-ABI serve calls (create, submit, step until done, destroy)"},
             "gpu_launches": tot["launches"], "clocks": clocks}
     if rank == 0 and ws == 1 and not args.no_extras:
-        line["kernels"] = kernel_comparison(E, torch, ctx, flush, local, nsm)
+        line["kernels"] = kernel_comparison(E, torch, ctx, flush, local, nsm, tuned)
         stream = serving_mix(E, ctx)
         serving_stats(E, ctx, stream)  # warm-up of the stream's job shapes
         line["serving"] = serving_stats(E, ctx, stream)
@@ -520,7 +552,7 @@ def main():
                                 "sample": sw["desc"] + " (4.0e9 steps)"}
         flush.zero_()
         torch.cuda.synchronize()
-        per, lines, ms, *_ = run_concurrent(E, ctx, make_jobs(E, sw))
+        per, lines, ms, *_ = run_concurrent(E, ctx, make_jobs(E, sw), tune)
         gsteps = sum(c.steps for c in per.values())
         line["same_sample"] = {"workload": sw["desc"], "gpu_steps_per_s": gsteps / (ms / 1000),
                                "cpu_steps_per_s": s / dt, "gpu_over_cpu": (gsteps / (ms / 1000)) / (s / dt),

@@ -13,7 +13,9 @@
    from per-probe streams (at most 2^20 probes), so the numbers are another
    sample of the same estimator: they equal the reference probe for probe, not
    line for line.  Environment: E13_DEVICE (CUDA device, default 0), E13_KERNEL
-   (persistent | plain).  There is no CPU path: without a GPU it exits 1.
+   (persistent | plain), E13_AUTOTUNE=N (tune the persistent kernel on 1/N of
+   the first job before searching; see maybe_autotune).  There is no CPU path:
+   without a GPU it exits 1.
 
    free / freesym keep checkpoints as src/e13gpu.py:349-409 does: E13_CKPT
    names the checkpoint (resumed when it exists), E13_CKPT_SEC the seconds
@@ -41,6 +43,26 @@ static e13_ctx *open_ctx(void) {
     exit(1);
   }
   return ctx;
+}
+
+/* E13_AUTOTUNE=N (N >= 1): before the first search, tune the persistent
+   kernel on shard 0 of N of that search's job (N = 1: the whole job) and use
+   the result for every search of the command. */
+static void maybe_autotune(e13_ctx *ctx, const e13_job *job, e13_tuning *tu) {
+  static int done = 0;
+  const char *a = getenv("E13_AUTOTUNE");
+  if (done || !a || atoi(a) < 1 || tu->kernel != E13_KERNEL_PERSISTENT) return;
+  done = 1;
+  e13_tuning best;
+  double ms = 0;
+  int rc = e13_autotune(ctx, job, atoi(a), tu, &best, &ms);
+  if (rc) {
+    fprintf(stderr, "autotune failed (error %d): default tuning kept\n", rc);
+    return;
+  }
+  fprintf(stderr, "autotune X=%d proxy=1/%d: block=%d slice=%d warp_stack=%d pool_low_pct=%d (%.1f ms)\n", job->X,
+          atoi(a), best.block, best.slice, best.warp_stack, best.pool_low_pct, ms);
+  *tu = best;
 }
 
 /* ck: NULL, or the checkpoint of a free / freesym run */
@@ -160,6 +182,7 @@ int main(int argc, char **argv) {
         fprintf(stderr, "X=%d: setup error %d\n", X, rc);
         return 1;
       }
+      maybe_autotune(ctx, &job, &tu);
       if (run_one(ctx, &job, &tu, NULL)) return 1;
     }
     e13_ctx_destroy(ctx);
@@ -202,6 +225,7 @@ int main(int argc, char **argv) {
     const char *cksec = getenv("E13_CKPT_SEC");
     e13_checkpoint ck = {ckpath, config, cksec ? atof(cksec) : 1800.0, 0.0};
     e13_ctx *ctx = open_ctx();
+    maybe_autotune(ctx, &job, &tu);
     rc = run_one(ctx, &job, &tu, (ckpath && ckpath[0]) ? &ck : NULL);
     e13_ctx_destroy(ctx);
     return rc == E13_STOPPED ? 3 : (rc ? 1 : 0);

@@ -1155,6 +1155,118 @@ static ShardKey shard_key(const Node &n) {
 constexpr long long kSplitPerShard = 512;  // frontier nodes per shard before the deal
 constexpr int kSplitLevels = 24;           // most plain launches of the split
 
+// One share of a search split over nshards (the reference's SPLIT frontier,
+// src/e13search.c:222-235, built for the device): the plain kernel expands the
+// job level by level, each launch taking the whole frontier, until it holds
+// kSplitPerShard nodes per shard; the frontier is then put in an order that
+// depends only on its nodes (the same on every rank) and shard s keeps nodes
+// s, s + nshards, ...  What the expansion itself finished (leaves, steps,
+// survivors, with their read masks) counts in shard 0 only: *cnt and *recs
+// are zero / empty for the other shards.  Runs on buffers of its own (freed
+// before it returns), so a serve session's frontier is left alone; `slot` is
+// the job slot written into the nodes.
+static int split_share(e13_ctx *c, const e13_job *job, const e13_tuning &tu, int shard, int nshards, int slot,
+                       std::vector<Node> &mine, unsigned long long cnt[kJobCounters], std::vector<SurvRec> &recs,
+                       long long *launches) {
+  mine.clear();
+  recs.clear();
+  memset(cnt, 0, sizeof(unsigned long long) * kJobCounters);
+  const long long nwarps = (long long)c->nsm * tu.block / 32;
+  const long long fan = 4LL * job->nq + 1;
+  const long long target = kSplitPerShard * nshards;
+  // the last level starts below target nodes and each node has at most `fan` children
+  const long long stack_n = target * fan + nwarps * 32 + 1024, out_n = stack_n, surv_n = 4096;
+  Node *stack = nullptr, *out = nullptr;
+  Ctl *ctl = nullptr;
+  JobParam *jobs = nullptr;
+  unsigned long long *jobcnt = nullptr;
+  SurvRec *surv = nullptr;
+  int rc = E13_OK;
+  auto fail = [&](cudaError_t e, const char *what) {
+    if (e != cudaSuccess && rc == E13_OK) rc = cuda_fail(e, what) ? E13_ERR_CUDA : E13_OK;
+    return rc != E13_OK;
+  };
+  JobParam jp[kMaxJobs];
+  memset(jp, 0, sizeof jp);
+  jp[slot].nv = 4 * job->nq;
+  jp[slot].sym_lo = job->sym_lo;
+  jp[slot].sym_hi = job->sym_hi;
+  Node root;
+  build_root(job, slot, &root, tu.run_skip != 0, true);
+  Ctl h;
+  memset(&h, 0, sizeof h);
+  h.top = 1;
+  h.batch = 1;
+  h.peak = 1;
+  long long top = 1;
+  if (!fail(cudaMalloc(&stack, sizeof(Node) * (size_t)stack_n), "split stack") &&
+      !fail(cudaMalloc(&out, sizeof(Node) * (size_t)out_n), "split outputs") &&
+      !fail(cudaMalloc(&ctl, sizeof(Ctl)), "split control") &&
+      !fail(cudaMalloc(&jobs, sizeof jp), "split job") &&
+      !fail(cudaMalloc(&jobcnt, sizeof(unsigned long long) * kMaxJobs * kJobCounters), "split counters") &&
+      !fail(cudaMalloc(&surv, sizeof(SurvRec) * (size_t)surv_n), "split survivors") &&
+      !fail(h2d(c, stack, &root, sizeof root), "split root") && !fail(h2d(c, ctl, &h, sizeof h), "split ctl") &&
+      !fail(h2d(c, jobs, jp, sizeof jp), "split job") &&
+      !fail(cudaMemsetAsync(jobcnt, 0, sizeof(unsigned long long) * kMaxJobs * kJobCounters, c->stream), "memset")) {
+    e13_tuning t = tu;
+    t.kernel = E13_KERNEL_PLAIN;
+    Params S = make_params(c, t, job->nq, nwarps, nwarps * 32);
+    S.jobs = jobs;
+    S.jobcnt = jobcnt;
+    S.stack = stack;
+    S.out = out;
+    S.out_cap = out_n;
+    S.out_soft = out_n;
+    S.surv = surv;
+    S.surv_cap = surv_n;
+    S.ctl = ctl;
+    const size_t smem = search_smem(tu.block);
+    fail(cudaFuncSetAttribute(search_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
+    for (int level = 0; rc == E13_OK && level < kSplitLevels && top > 0 && top < target; ++level) {
+      search_kernel<false><<<c->nsm, tu.block, smem, c->stream>>>(S);
+      move_outputs<<<c->nsm * 4, 256, 0, c->stream>>>(ctl, stack, out, c->pool, 0, stack_n);
+      finish_launch<<<1, 1, 0, c->stream>>>(ctl, stack_n, kWholeFrontier, 0);
+      *launches += 3;
+      if (fail(cudaGetLastError(), "split launch") || fail(d2h(c, &h, ctl, sizeof h), "split ctl") ||
+          fail(cudaStreamSynchronize(c->stream), "split sync"))
+        break;
+      if (h.error) rc = E13_ERR_OVERFLOW;
+      top = h.top;
+    }
+  }
+  if (rc == E13_OK) {
+    // the deal
+    std::vector<Node> nodes((size_t)top);
+    const long long nrec = std::min<long long>((long long)h.nsurv, surv_n);
+    if (shard == 0 && nrec > 0) {
+      survivor_read_masks<<<(unsigned)((nrec + 31) / 32), 32, 0, c->stream>>>(surv, nrec);
+      recs.resize((size_t)nrec);
+      fail(cudaGetLastError(), "split survivors");
+      if (rc == E13_OK) fail(d2h(c, recs.data(), surv, sizeof(SurvRec) * (size_t)nrec), "split survivors");
+    }
+    if (rc == E13_OK && top > 0) fail(d2h(c, nodes.data(), stack, sizeof(Node) * (size_t)top), "split frontier");
+    if (rc == E13_OK && shard == 0)
+      fail(d2h(c, cnt, jobcnt + (size_t)slot * kJobCounters, sizeof(unsigned long long) * kJobCounters), "counters");
+    if (rc == E13_OK) fail(cudaStreamSynchronize(c->stream), "split sync");
+    if (rc == E13_OK && (long long)h.nsurv > surv_n) rc = E13_ERR_SURV_CAP;
+    if (rc == E13_OK) {
+      std::vector<std::pair<ShardKey, long long>> order((size_t)top);
+      for (long long i = 0; i < top; ++i) order[(size_t)i] = {shard_key(nodes[(size_t)i]), i};
+      std::sort(order.begin(), order.end(), [](const std::pair<ShardKey, long long> &a,
+                                               const std::pair<ShardKey, long long> &b) { return a.first < b.first; });
+      for (long long i = shard; i < top; i += nshards) mine.push_back(nodes[(size_t)order[(size_t)i].second]);
+    }
+  }
+  cudaStreamSynchronize(c->stream);
+  cudaFree(stack);
+  cudaFree(out);
+  cudaFree(ctl);
+  cudaFree(jobs);
+  cudaFree(jobcnt);
+  cudaFree(surv);
+  return rc;
+}
+
 static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning, const e13_checkpoint *ck,
                        e13_counts *counts, e13_survivor *surv, int surv_cap, int *nsurv, double *wall_s,
                        int64_t *frontier, int shard = 0, int nshards = 1) {
@@ -1266,53 +1378,21 @@ static int search_impl(e13_ctx *c, const e13_job *job, const e13_tuning *tuning,
   bool split = false;
   if (nshards > 1) {
     split = true;
-    Params S = P;
-    CK(cudaFuncSetAttribute(search_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    long long top = 1;
-    for (int level = 0; level < kSplitLevels && top > 0 && top < kSplitPerShard * nshards; ++level) {
-      const long long need = top * (4LL * job->nq + 1) + nwarps * 32 + 1024;
-      if (need > c->out_cap) {
-        CK(cudaStreamSynchronize(c->stream));
-        if ((rc = grow(&c->out, &c->out_cap, need))) return rc;
-      }
-      S.out = c->out;
-      S.out_cap = c->out_cap;
-      search_kernel<false><<<blocks, tu.block, smem, c->stream>>>(S);
-      move_outputs<<<move_blocks, 256, 0, c->stream>>>(c->ctl, c->stack, c->out, c->pool, c->pool_cap, cap);
-      finish_launch<<<1, 1, 0, c->stream>>>(c->ctl, cap, kWholeFrontier, c->pool_cap);
-      launches += 3;
-      search_launches += 1;
-      CK(cudaGetLastError());
-      CK(d2h(c, c->ctl_host, c->ctl, sizeof(Ctl)));
-      CK(cudaStreamSynchronize(c->stream));
-      if (c->ctl_host->error) return E13_ERR_OVERFLOW;
-      top = c->ctl_host->top;
-    }
-    // the deal
-    std::vector<Node> nodes((size_t)top);
-    if (top > 0)
-      CK(d2h(c, nodes.data(), c->stack, sizeof(Node) * (size_t)top));
-    CK(cudaStreamSynchronize(c->stream));
-    std::vector<std::pair<ShardKey, long long>> order((size_t)top);
-    for (long long i = 0; i < top; ++i) order[(size_t)i] = {shard_key(nodes[(size_t)i]), i};
-    std::sort(order.begin(), order.end(), [](const std::pair<ShardKey, long long> &a,
-                                             const std::pair<ShardKey, long long> &b) { return a.first < b.first; });
     std::vector<Node> mine;
-    for (long long i = shard; i < top; i += nshards) mine.push_back(nodes[(size_t)order[(size_t)i].second]);
-    if (!mine.empty())
-      CK(h2d(c, c->stack, mine.data(), sizeof(Node) * mine.size()));
+    std::vector<SurvRec> recs;
+    unsigned long long cnt[kJobCounters];
+    if ((rc = split_share(c, job, tu, shard, nshards, 0, mine, cnt, recs, &launches))) return rc;
+    search_launches += launches / 3;
+    if ((long long)mine.size() > cap - out_nodes) return E13_ERR_OVERFLOW;
+    if (!mine.empty()) CK(h2d(c, c->stack, mine.data(), sizeof(Node) * mine.size()));
+    if (!recs.empty()) CK(h2d(c, c->surv, recs.data(), sizeof(SurvRec) * recs.size()));
+    CK(h2d(c, c->d_jobcnt, cnt, sizeof cnt));
     c->ctl_host->top = (long long)mine.size();
     c->ctl_host->batch = std::min<long long>((long long)mine.size(), batch_max);
-    if (shard != 0) {
-      c->ctl_host->nsurv = 0;
-      CK(cudaMemsetAsync(c->d_jobcnt, 0, sizeof(unsigned long long) * kMaxJobs * kJobCounters, c->stream));
-    }
+    c->ctl_host->peak = c->ctl_host->top;
+    c->ctl_host->nsurv = recs.size();
     CK(h2d(c, c->ctl, c->ctl_host, sizeof(Ctl)));
     CK(cudaStreamSynchronize(c->stream));
-    // the split may have grown the output buffer: the main phase uses the new one
-    P.out = c->out;
-    P.out_cap = c->out_cap;
-    P.out_soft = c->out_cap - dump_room - 1024;
   }
   if (persist) {
     cudaGraph_t graph;
@@ -1500,31 +1580,43 @@ extern "C" int e13_selftest_pool_wait(e13_ctx *c, int32_t wait_us) {
 // ------------------------------------------------------------------------
 // autotuner
 
-extern "C" int e13_autotune(e13_ctx *c, const e13_job *job, const e13_tuning *start, e13_tuning *best,
-                            double *best_ms) {
-  if (!c || !job || !best) return E13_ERR_ARG;
+extern "C" int e13_autotune(e13_ctx *c, const e13_job *job, int32_t proxy_shards, const e13_tuning *start,
+                            e13_tuning *best, double *best_ms) {
+  if (!c || !job || !best || proxy_shards < 0 || proxy_shards > 4096) return E13_ERR_ARG;
   e13_tuning cur;
-  if (start) cur = *start;
-  else e13_default_tuning(&cur);
+  if (e13_resolve_tuning(start, 0, &cur) != E13_OK) return E13_ERR_ARG;
   cur.kernel = E13_KERNEL_PERSISTENT;
+  const int nsh = proxy_shards > 1 ? proxy_shards : 1;
   e13_counts ref_counts, got;
   int ns = 0;
   std::vector<e13_survivor> surv(4096);
-  // every candidate must give the same totals: a free determinism check
-  int rc = e13_search(c, job, &cur, &ref_counts, surv.data(), (int)surv.size(), &ns);
-  if (rc && rc != E13_ERR_SURV_CAP) return rc;
-  double cur_ms = c->stats.device_ms;
+  // the proxy: shard 0 of the job's own subtrees (e13_search_shard), so the
+  // tuning is timed on the job's own mix of machines at a fraction of its cost
+  auto run = [&](const e13_tuning &t, e13_counts *out, double *ms) -> int {
+    const int rc = e13_search_shard(c, job, &t, 0, nsh, out, surv.data(), (int)surv.size(), &ns);
+    if (rc && rc != E13_ERR_SURV_CAP) return rc;
+    *ms = c->stats.device_ms;
+    return E13_OK;
+  };
+  double cur_ms = 0;
+  int rc = run(cur, &ref_counts, &cur_ms);  // warms the buffers up
+  if (rc) return rc;
+  if ((rc = run(cur, &got, &cur_ms))) return rc;
+  if (memcmp(&got, &ref_counts, sizeof got) != 0) return E13_ERR_CUDA;
   struct Axis {
     int32_t e13_tuning::*field;
-    int vals[4];
+    int vals[5];
     int n;
   };
+  // block: lanes per CTA (one CTA per SM); slice: actions between a warp's
+  // refill rounds; warp_stack: the depth of subtree a warp keeps to itself
+  // before it spills or donates; pool_low_pct: the threshold below which warps
+  // with deep stacks fork work off to idle warps
   const Axis axes[] = {
-      {&e13_tuning::block, {512, 640, 768, 0}, 3},
-      {&e13_tuning::slice, {16, 32, 64, 128}, 4},
-      {&e13_tuning::warp_stack, {64, 128, 256, 512}, 4},
-      {&e13_tuning::batch, {0, 65536, 1 << 20, 0}, 3},
-      {&e13_tuning::pool_low_pct, {5, 12, 25, 50}, 4},
+      {&e13_tuning::block, {512, 640, 768, 0, 0}, 3},
+      {&e13_tuning::slice, {12, 16, 24, 32, 48}, 5},
+      {&e13_tuning::warp_stack, {64, 128, 256, 512, 0}, 4},
+      {&e13_tuning::pool_low_pct, {2, 5, 12, 25, 0}, 4},
   };
   for (const Axis &ax : axes) {
     e13_tuning axis_best = cur;
@@ -1533,11 +1625,11 @@ extern "C" int e13_autotune(e13_ctx *c, const e13_job *job, const e13_tuning *st
       if (ax.vals[i] == cur.*(ax.field)) continue;
       e13_tuning t = cur;
       t.*(ax.field) = ax.vals[i];
-      rc = e13_search(c, job, &t, &got, surv.data(), (int)surv.size(), &ns);
-      if (rc && rc != E13_ERR_SURV_CAP) return rc;
+      double ms = 0;
+      if ((rc = run(t, &got, &ms))) return rc;
       if (memcmp(&got, &ref_counts, sizeof got) != 0) return E13_ERR_CUDA;  // results must not depend on tuning
-      if (c->stats.device_ms < axis_ms) {
-        axis_ms = c->stats.device_ms;
+      if (ms < axis_ms * 0.98) {  // a 2 % margin keeps timing noise from moving the choice
+        axis_ms = ms;
         axis_best = t;
       }
     }
@@ -1687,6 +1779,31 @@ extern "C" int e13_serve_submit(e13_serve *s, const e13_job *job, int64_t id, do
     j->reserve = tree * 2.0 < (double)s->large_reserve ? std::max<long long>(64, (long long)(tree * 2.0) + 1)
                                                        : s->large_reserve;
   }
+  s->queue.push_back(std::move(j));
+  return E13_OK;
+}
+
+extern "C" int e13_serve_submit_shard(e13_serve *s, const e13_job *job, int64_t id, double t_submit, int shard,
+                                      int nshards) {
+  if (!s || !job || nshards < 1 || shard < 0 || shard >= nshards) return E13_ERR_ARG;
+  if (nshards == 1) return e13_serve_submit(s, job, id, t_submit);
+  int rc = e13_serve_submit(s, job, id, t_submit);  // checks the job and sizes it
+  if (rc) return rc;
+  std::unique_ptr<ServeJob> j = std::move(s->queue.back());
+  s->queue.pop_back();
+  std::vector<SurvRec> recs;
+  long long launches = 0;
+  CK(cudaSetDevice(s->c->device));
+  if ((rc = split_share(s->c, job, s->tu, shard, nshards, 0, j->saved, j->saved_cnt, recs, &launches))) return rc;
+  s->c->stats.launches += launches;
+  for (const SurvRec &r : recs) {
+    e13_survivor sv;
+    decode_survivor(r, job->nq, &sv);
+    j->surv.push_back(sv);
+  }
+  // it starts as a job swapped out with its share of the frontier
+  j->swapped = true;
+  j->reserve = std::max<long long>({64, j->reserve / nshards, 2 * (long long)j->saved.size()});
   s->queue.push_back(std::move(j));
   return E13_OK;
 }

@@ -157,6 +157,7 @@ def lib():
         L.e13_serve_clock.restype = ctypes.c_double
         L.e13_serve_submit.argtypes = [ctypes.c_void_p, P(Job), ctypes.c_int64, ctypes.c_double]
         L.e13_serve_step.argtypes = [ctypes.c_void_p, P(ServeResult), I, P(I)]
+        L.e13_serve_submit_shard.argtypes = [ctypes.c_void_p, P(Job), ctypes.c_int64, ctypes.c_double, I, I]
         L.e13_serve_pending.argtypes = [ctypes.c_void_p]
         L.e13_serve_pending.restype = ctypes.c_int64
         L.e13_serve_survivors.argtypes = [ctypes.c_void_p, ctypes.c_int64, P(Survivor), I, P(I)]
@@ -179,7 +180,7 @@ EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine
             "e13_format_recheck", "e13_format_deep", "e13_check_crafted", "e13_raw_run", "e13_autotune", "e13_check_noalloc",
             "e13_serve_create", "e13_serve_destroy", "e13_serve_clock", "e13_serve_submit", "e13_serve_step",
             "e13_serve_pending", "e13_serve_survivors", "e13_serve_stats", "e13_resolve_tuning",
-            "e13_selftest_pool_wait"]
+            "e13_selftest_pool_wait", "e13_serve_submit_shard"]
 
 
 def keys():
@@ -329,12 +330,13 @@ class Context:
             return buf.value.decode().splitlines()
         raise E13Error(-1, "e13_check_crafted")
 
-    def autotune(self, job: Job, start: Tuning | None = None):
-        """Coordinate-descent tuning of the persistent kernel on `job`; returns (Tuning, best ms)."""
+    def autotune(self, job: Job, start: Tuning | None = None, proxy_shards: int = 1):
+        """Coordinate-descent tuning of the persistent kernel, timed on shard 0 of
+        proxy_shards of `job`; returns (Tuning, best proxy ms)."""
         best = Tuning()
         ms = ctypes.c_double()
-        r = lib().e13_autotune(self.h, ctypes.byref(job), ctypes.byref(start) if start else None, ctypes.byref(best),
-                               ctypes.byref(ms))
+        r = lib().e13_autotune(self.h, ctypes.byref(job), proxy_shards, ctypes.byref(start) if start else None,
+                               ctypes.byref(best), ctypes.byref(ms))
         if r:
             raise E13Error(r, "e13_autotune")
         return best, ms.value
@@ -450,6 +452,11 @@ class Server:
         if r:
             raise E13Error(r, "e13_serve_submit")
 
+    def submit_shard(self, job: Job, job_id: int, shard: int, nshards: int, t_submit: float = -1.0):
+        r = lib().e13_serve_submit_shard(self.h, ctypes.byref(job), job_id, t_submit, shard, nshards)
+        if r:
+            raise E13Error(r, "e13_serve_submit_shard")
+
     def step(self):
         res = (ServeResult * 16)()
         n = ctypes.c_int()
@@ -482,11 +489,16 @@ class Server:
         lib().e13_serve_stats(self.h, None, None, ctypes.byref(n))
         return n.value
 
-    def run_all(self, jobs, arrivals=None):
-        """Submits jobs (with optional arrival times) and steps until all are
-        done; returns {id: (ServeResult, [Survivor])}."""
+    def run_all(self, jobs, arrivals=None, shard=0, nshards=1):
+        """Submits jobs (with optional arrival times; with nshards > 1 this
+        rank's share of each) and steps until all are done; returns
+        {id: (ServeResult, [Survivor])}."""
         for i, job in enumerate(jobs):
-            self.submit(job, i, -1.0 if arrivals is None else arrivals[i])
+            t = -1.0 if arrivals is None else arrivals[i]
+            if nshards > 1:
+                self.submit_shard(job, i, shard, nshards, t)
+            else:
+                self.submit(job, i, t)
         out = {}
         while self.pending():
             for r in self.step():

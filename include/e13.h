@@ -305,6 +305,14 @@ double e13_serve_clock(const e13_serve *s);
 /* Queues a job; t_submit < 0 means now (serve clock).  Unless the session has
    a fixed reservation, runs the job's size estimate on the device first. */
 int e13_serve_submit(e13_serve *s, const e13_job *job, int64_t id, double t_submit);
+/* Queues one share of a job split over nshards (shard in [0, nshards)), for
+   spreading a set of jobs over GPUs with one serve session per GPU: the job's
+   frontier is expanded and dealt out as e13_search_shard does, the share then
+   joins this session like any job, and the counts and survivors of all shards
+   of a job add up to the job's.  The expansion runs here, on the device and on
+   buffers of its own, before the call returns.  nshards = 1 is
+   e13_serve_submit. */
+int e13_serve_submit_shard(e13_serve *s, const e13_job *job, int64_t id, double t_submit, int shard, int nshards);
 /* One admission + epoch + completion pass; done needs room for 16 results. */
 int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int *ndone);
 /* Jobs queued or running. */
@@ -316,14 +324,20 @@ int e13_serve_survivors(e13_serve *s, int64_t id, e13_survivor *out, int cap, in
 int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs, int64_t *swapped_out);
 
 /* Autotuner (no counterpart in the reference, which has one fixed GPU
-   launch shape): coordinate descent over block size (lanes per CTA), slice
-   (steps between refills), warp_stack (subtree depth kept private to a warp
-   before it spills to the frontier) and pool_low_pct (donation threshold),
-   timing the persistent kernel on `job` with CUDA events.  Use a job that runs
-   in well under a second as the proxy for a larger one.  Every candidate must
-   reproduce the same counts, else E13_ERR_CUDA.  start may be NULL
-   (defaults); *best_ms (may be NULL) is the best device time. */
-int e13_autotune(e13_ctx *ctx, const e13_job *job, const e13_tuning *start, e13_tuning *best, double *best_ms);
+   launch shape, src/e13gpu.py:342-346, and a fixed serial split depth,
+   E13_SPLIT, src/e13search.c:47-49): coordinate descent over block size
+   (lanes per CTA, one CTA per SM), slice (actions between a warp's refill
+   rounds), warp_stack (the subtree depth a warp keeps to itself before it
+   spills to the frontier or donates) and pool_low_pct (the donation
+   threshold at which warps with deep stacks fork work off to idle warps),
+   timing the persistent kernel with CUDA events.  The proxy is shard 0 of
+   proxy_shards of the job itself (e13_search_shard; 0 or 1 = the whole job), so
+   a candidate costs about 1/proxy_shards of the job.  Each axis keeps a value
+   only if it is at least 2 % faster.  Every candidate must reproduce the same
+   counts, else E13_ERR_CUDA.  start may be NULL (defaults); *best_ms (may be
+   NULL) is the best proxy time. */
+int e13_autotune(e13_ctx *ctx, const e13_job *job, int32_t proxy_shards, const e13_tuning *start, e13_tuning *best,
+                 double *best_ms);
 
 /* Self-test of the persistent kernel's one device-side wait, for a caller
    (or a test) that wants to see a device wait run out without a hang: runs

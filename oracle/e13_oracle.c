@@ -404,12 +404,29 @@ static void *pool_worker(void *arg) {
   return NULL;
 }
 
+/* One share of the search, split the way the reference splits a search over
+   threads (e13search.c:222-235, 376-403): a serial walk collects the machines
+   at their second branching first read; frontier node k belongs to shard
+   k % nshards, and what the serial walk finished itself (leaves, steps,
+   survivors) counts in shard 0 only.  So the shards' counts add up to the
+   whole search and their survivors together are its survivors.  Arguments
+   and outputs as oracle_search. */
+int oracle_search_shard(const int *tab0, int nq, int budget, int sym_lo, int sym_hi, int sym_n0, int nthreads,
+                        int shard, int nshards, long long *counts_out, int *surv, int surv_cap, int *nsurv);
+
 /* The whole search for one prepared table.  counts_out: leaves, survivors,
    steps, hist[0..9] (13 long longs).  Survivor records (O_REC ints each) go
    to surv (up to surv_cap); *nsurv gets the total found.  nthreads <= 1 runs
    serially. */
 int oracle_search(const int *tab0, int nq, int budget, int sym_lo, int sym_hi, int sym_n0, int nthreads,
                   long long *counts_out, int *surv, int surv_cap, int *nsurv) {
+  return oracle_search_shard(tab0, nq, budget, sym_lo, sym_hi, sym_n0, nthreads, 0, 1, counts_out, surv, surv_cap,
+                             nsurv);
+}
+
+int oracle_search_shard(const int *tab0, int nq, int budget, int sym_lo, int sym_hi, int sym_n0, int nthreads,
+                        int shard, int nshards, long long *counts_out, int *surv, int surv_cap, int *nsurv) {
+  if (nshards < 1 || shard < 0 || shard >= nshards) return -1;
   oracle_keys(NULL, NULL);
   pthread_mutex_t lock = PTHREAD_MUTEX_INITIALIZER, qlock = PTHREAD_MUTEX_INITIALIZER;
   int shared_n = 0;
@@ -424,11 +441,21 @@ int oracle_search(const int *tab0, int nq, int budget, int sym_lo, int sym_hi, i
   top->surv_cap = surv_cap;
   top->lock = &lock;
   top->surv_shared_n = &shared_n;
-  top->collect_depth = nthreads > 1 ? 2 : -1;
+  top->collect_depth = (nthreads > 1 || nshards > 1) ? 2 : -1;
   osim_blank(&top->stack_sims[0]);
   walk(top, 0, tab, read, budget, sym_n0, 0);
   OCounts total = top->c;
-  if (nthreads > 1 && top->nfront > 0) {
+  if (shard != 0) {
+    memset(&total, 0, sizeof total); /* the serial walk's own results belong to shard 0 */
+    shared_n = 0;
+  }
+  if (nshards > 1) { /* keep this shard's frontier nodes, in collection order */
+    long n = 0;
+    for (long k = shard; k < top->nfront; k += nshards) top->front[n++] = top->front[k];
+    top->nfront = n;
+  }
+  if (top->collect_depth >= 0 && top->nfront > 0) {
+    if (nthreads < 1) nthreads = 1;
     long next = 0;
     pthread_t *th = (pthread_t *)calloc((size_t)nthreads, sizeof(pthread_t));
     OWalk *ws = (OWalk *)calloc((size_t)nthreads, sizeof(OWalk));

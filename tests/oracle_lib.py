@@ -39,6 +39,7 @@ def lib():
         L.oracle_load.argtypes = [ctypes.c_char_p, P(I)]
         L.oracle_setup.argtypes = [P(I), I, I, I, ctypes.c_char_p, I, I, P(I), P(I), P(I), P(I), P(I)]
         L.oracle_search.argtypes = [P(I), I, I, I, I, I, I, P(ctypes.c_longlong), P(I), I, P(I)]
+        L.oracle_search_shard.argtypes = [P(I), I, I, I, I, I, I, I, I, P(ctypes.c_longlong), P(I), I, P(I)]
         L.oracle_run_full.argtypes = [P(I), I, P(ctypes.c_longlong)]
         L.oracle_recheck_line.argtypes = [ctypes.c_char_p, I, ctypes.c_char_p, I, ctypes.c_char_p, I]
         L.oracle_deep_line.argtypes = [ctypes.c_char_p, I, ctypes.c_char_p, I]
@@ -107,14 +108,15 @@ def setup(base, X, fmax=0, free_cells=None, lo=-1, hi=-1):
     return r, Job(list(tab)[: 2 * nq], nq, r, slo.value, shi.value, n0.value, nf.value, X)
 
 
-def search(job: Job, nthreads: int = 8, surv_cap: int = 100000):
-    """Runs the oracle search; returns (counts dict, list of survivor records)."""
+def search(job: Job, nthreads: int = 8, surv_cap: int = 100000, shard: int = 0, nshards: int = 1):
+    """Runs the oracle search (with nshards > 1, one share of it, see
+    oracle_search_shard); returns (counts dict, list of survivor records)."""
     tab = (ctypes.c_int * 32)(*(job.tab + [HALT] * (32 - len(job.tab))))
     counts = (ctypes.c_longlong * 13)()
     surv = (ctypes.c_int * (REC_INTS * surv_cap))()
     ns = ctypes.c_int()
-    lib().oracle_search(tab, job.nq, max(job.budget, 0), job.sym_lo, job.sym_hi, job.sym_n0, nthreads, counts,
-                        surv, surv_cap, ctypes.byref(ns))
+    lib().oracle_search_shard(tab, job.nq, max(job.budget, 0), job.sym_lo, job.sym_hi, job.sym_n0, nthreads, shard,
+                              nshards, counts, surv, surv_cap, ctypes.byref(ns))
     c = list(counts)
     recs = []
     for k in range(min(ns.value, surv_cap)):

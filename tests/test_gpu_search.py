@@ -202,14 +202,21 @@ def test_run_full_matches_oracle_random_tables():
 
 
 def test_autotune_keeps_results(searches):
-    """The autotuner times candidate launch shapes on a proxy job; every
-    candidate must reproduce the same counts, and the tuning it returns too."""
+    """The autotuner times candidate launch shapes on shard 0 of 4 of a job;
+    every candidate must reproduce the same counts, and the tuning it returns
+    gives the golden totals on the whole job, on both the search and a serve
+    session."""
     e = searches["local_edits_f3"]
     job = __import__("gpu_common").make_job(e, 12)
-    best, ms = ctx().autotune(job)
-    assert ms > 0 and best.block in (512, 640, 768)
+    best, ms = ctx().autotune(job, proxy_shards=4)
+    assert ms > 0 and best.block in (512, 640, 768) and best.slice in (12, 16, 24, 32, 48)
+    assert best.warp_stack in (64, 128, 256, 512) and best.pool_low_pct in (2, 5, 12, 25)
     c, _ = ctx().search(job, best)
-    assert c.as_dict()["leaves"] == e["expect"][12]["leaves"]
+    exp = e["expect"][12]
+    assert c.leaves == exp["leaves"] and list(c.hist) == exp["hist"] and c.steps == exp["steps"]
+    with E.Server(ctx(), best) as srv:
+        got = srv.run_all([job])
+    assert got[0][0].counts.leaves == exp["leaves"]
 
 
 def _budget_symmetry_cases(n, seed):

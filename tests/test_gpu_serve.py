@@ -74,3 +74,74 @@ def test_big_and_small_jobs_interleave(searches):
         check_entry(dict(e, expect=[_expect(e, X)]), [res.counts.as_dict()])
     res, surv = got[len(mix) - 1]
     assert sorted(E.survivor_line(jobs[-1], s) for s in surv) == golden_lines(searches["counter_sym"])
+
+
+def test_swap_out_keeps_results(searches):
+    """A frontier capacity too small for the jobs running together: after an
+    epoch the jobs with the most live nodes are swapped out to host memory and
+    resumed later.  Every job's counts and survivors still equal the
+    reference's; at least one swap happened."""
+    mix = [(searches["local_edits_f3"], X) for X in range(14)] + [(searches["counter_sym"], 13)]
+    jobs = [make_job(e, X) for e, X in mix]
+    # small launch shape: one epoch's outputs need 2 * 1184 * 48 + 65536 nodes of room
+    tune = E.tuning(block=256, warp_stack=16, stack_nodes=2 * 1184 * 48 + 65536 + 60000, epoch_us=5000)
+    with E.Server(ctx(), tune) as srv:
+        got = srv.run_all(jobs)
+        swaps = srv.swapped_out()
+    assert swaps > 0
+    for i, (e, X) in enumerate(mix):
+        res, surv = got[i]
+        assert res.status == 0, (X, res.status)
+        check_entry(dict(e, expect=[_expect(e, X)]), [res.counts.as_dict()])
+    res, surv = got[len(mix) - 1]
+    assert sorted(E.survivor_line(jobs[-1], s) for s in surv) == golden_lines(searches["counter_sym"])
+
+
+def test_admission_reserves_by_estimate(searches):
+    """With estimate-based reservations many small jobs run at once next to a
+    large one; with a fixed reservation of the whole capacity they run one at
+    a time.  Results are the same either way."""
+    mix = [(searches["local_edits_f2"], X) for X in range(14)]
+    jobs = [make_job(e, X) for e, X in mix]
+    tune = E.tuning(stack_nodes=8 << 20)
+    with E.Server(ctx(), tune) as srv:
+        got = srv.run_all(jobs)
+        _, ep_est = srv.stats()
+    with E.Server(ctx(), tune, reserve_nodes=8 << 20) as srv:
+        got_fixed = srv.run_all(jobs)
+        _, ep_fixed = srv.stats()
+    assert ep_est < ep_fixed
+    for i, (e, X) in enumerate(mix):
+        assert got[i][0].counts.as_dict() == got_fixed[i][0].counts.as_dict()
+        check_entry(dict(e, expect=[_expect(e, X)]), [got[i][0].counts.as_dict()])
+
+
+@pytest.mark.parametrize("nshards", [2, 3])
+def test_serve_shards_add_up(searches, nshards):
+    """e13_serve_submit_shard: the shards of each job, run as separate jobs of
+    one session, add up to the reference's counts, and their survivors together
+    are the job's."""
+    cases = [(searches["local_edits_f3"], 11), (searches["counter_sym"], 13), (searches["local_edits_f2"], 8)]
+    with E.Server(ctx()) as srv:
+        for k, (e, X) in enumerate(cases):
+            job = make_job(e, X)
+            for sh in range(nshards):
+                srv.submit_shard(job, 100 * k + sh, sh, nshards)
+        out = {}
+        while srv.pending():
+            for r in srv.step():
+                out[r.id] = (r, srv.survivors(r.id))
+    for k, (e, X) in enumerate(cases):
+        job = make_job(e, X)
+        tot = None
+        lines = []
+        for sh in range(nshards):
+            r, surv = out[100 * k + sh]
+            assert r.status == 0
+            d = r.counts.as_dict()
+            tot = d if tot is None else {f: ([a + b for a, b in zip(tot[f], v)] if f == "hist" else tot[f] + v)
+                                         for f, v in d.items()}
+            lines += [E.survivor_line(job, s) for s in surv]
+        check_entry(dict(e, expect=[_expect(e, X)]), [tot])
+        want = [l for l in golden_lines(e) if l.startswith(f"SURVIVOR X={X} ")]
+        assert sorted(lines) == want

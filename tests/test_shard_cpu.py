@@ -78,6 +78,57 @@ def test_sharded_f2_equals_whole_run(searches, world):
         assert lines == gold
 
 
+def _rank_main_subtrees(rank, world, port, entry, q):
+    """Every rank searches shard `rank` of `world` of every job (the oracle's
+    subtree split: the serial walk's own leaves count in shard 0 only), then
+    the ranks sum the per-job counts and gather the survivor lines."""
+    import torch.distributed as dist
+
+    import e13shard as S
+    import oracle_lib as O
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, init_method=f"tcp://127.0.0.1:{port}",
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        base = O.load_machine(entry["machine"])
+        per, lines, shard0 = {}, [], {}
+        for X in entry["X"]:
+            r, job = O.setup(base, X, fmax=entry["fmax"])
+            c, recs = O.search(job, nthreads=2, shard=rank, nshards=world)
+            per[X] = c
+            lines += [O.survivor_line(X, rec, job.nq) for rec in recs]
+        q.put((rank, per, S.sum_counts(dist, per), S.gather_lines(dist, lines)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_subtree_sharded_f2_equals_whole_run(searches, world):
+    """The split the sharded bench uses: every rank takes its share of every
+    job; the per-job sums over ranks equal the reference's per-X log lines and
+    the gathered survivor lines its survivor file.  Each rank's share is a
+    proper part: no rank alone has a whole job's leaves."""
+    entry = searches["local_edits_f2"]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main_subtrees, args=(r, world, port, entry, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    gold = golden_lines(entry)
+    exp = {e["X"]: e for e in entry["expect"]}
+    for rank, per, summed, lines in got:
+        assert lines == gold
+        for X, e in exp.items():
+            assert summed[X] == {k: e[k] for k in ("leaves", "survivors", "steps", "hist")}, (rank, X)
+    big = max(exp, key=lambda X: exp[X]["leaves"])
+    assert all(per[big]["leaves"] < exp[big]["leaves"] for _, per, _, _ in got)
+
+
 def test_share_rejects_bad_rank():
     import e13shard as S
 
