@@ -1691,6 +1691,7 @@ struct e13_serve {
   double t0;
   double device_ms;
   long long epochs, evictions;
+  long long peak_top, peak_job;  // largest frontier after an epoch, and one job's largest share of it
   // frontier order between epochs: a second stack buffer, the group starts
   Node *alt = nullptr;
   long long alt_cap = 0;
@@ -1862,6 +1863,68 @@ static int set_top(e13_serve *s, long long top) {
   return E13_OK;
 }
 
+// Swaps jobs out of the frontier: order[0..first) leave it, order[first..n)
+// stay (most live nodes first, the usual order).  The frontier is regrouped
+// bottom to top as the staying jobs, then the leaving ones, whose nodes are
+// then copied to host memory from above the new top (`after` nodes).  Each
+// leaving job takes its counters (cnt, as of the last epoch) and goes back to
+// the head of the queue, reserving at least twice the nodes it had; a slot
+// already emptied (a job that failed) only has its nodes dropped.
+static int swap_out(e13_serve *s, const int *order, int n, int first, const unsigned long long *nodes,
+                    const unsigned long long *cnt, long long after) {
+  e13_ctx *c = s->c;
+  int lay[kMaxJobs], m = 0;
+  for (int i = first; i < n; ++i) lay[m++] = order[i];
+  for (int i = first - 1; i >= 0; --i) lay[m++] = order[i];
+  int rc;
+  if ((rc = regroup(s, lay, m, nodes))) return rc;
+  long long pos = after;
+  for (int i = first - 1; i >= 0; --i) {
+    const int k = order[i];
+    if (s->slot_job[k]) {
+      std::unique_ptr<ServeJob> j = std::move(s->slot_job[k]);
+      j->saved.resize((size_t)nodes[k]);
+      if (nodes[k]) CK(d2h(c, j->saved.data(), c->stack + pos, sizeof(Node) * (size_t)nodes[k]));
+      memcpy(j->saved_cnt, cnt + k * kJobCounters, sizeof j->saved_cnt);
+      j->swapped = true;
+      j->reserve = std::max<long long>(j->reserve, 2 * (long long)nodes[k]);
+      j->slot = -1;
+      s->queue.push_front(std::move(j));
+      ++s->evictions;
+    }
+    pos += (long long)nodes[k];
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  s->reorder = false;  // the staying jobs are in order already
+  return set_top(s, after);
+}
+
+extern "C" int e13_serve_preempt(e13_serve *s, int64_t id) {
+  if (!s) return E13_ERR_ARG;
+  for (const auto &q : s->queue)
+    if (q->id == id) return E13_OK;  // queued (or swapped out already): nothing to do
+  int slot = -1;
+  for (int k = 0; k < kMaxJobs; ++k)
+    if (s->slot_job[k] && s->slot_job[k]->id == id) slot = k;
+  if (slot < 0) return E13_ERR_ARG;  // unknown or finished
+  e13_ctx *c = s->c;
+  CK(cudaSetDevice(c->device));
+  // node counts and counters as the last epoch left them (nothing ran since)
+  const unsigned long long *cnt = c->h_jobbuf, *nodes = c->h_jobbuf + kMaxJobs * kJobCounters;
+  int order[kMaxJobs], n = 0;
+  unsigned long long accounted = 0;
+  order[n++] = slot;
+  for (int k = 0; k < kMaxJobs; ++k)
+    if (k != slot && s->slot_job[k] && nodes[k] > 0) order[n++] = k;
+  for (int i = 0; i < n; ++i) accounted += nodes[order[i]];
+  if (accounted != (unsigned long long)c->ctl_host->top) return E13_ERR_ARG;
+  std::sort(order + 1, order + n, [&](int a, int b) {
+    if (nodes[a] != nodes[b]) return nodes[a] > nodes[b];
+    return s->slot_job[a]->t_start < s->slot_job[b]->t_start;
+  });
+  return swap_out(s, order, n, 1, nodes, cnt, c->ctl_host->top - (long long)nodes[slot]);
+}
+
 extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int *ndone) {
   if (!s || !ndone || (cap > 0 && !done) || cap < kMaxJobs) return E13_ERR_ARG;
   *ndone = 0;
@@ -1979,6 +2042,9 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
   // 4. jobs with no node left are done
   const double tdone = e13_serve_clock(s);
   const unsigned long long *cnt = c->h_jobbuf, *nodes = c->h_jobbuf + kMaxJobs * kJobCounters;
+  s->peak_top = std::max<long long>(s->peak_top, c->ctl_host->top);
+  for (int k = 0; k < kMaxJobs; ++k)
+    if (s->slot_job[k]) s->peak_job = std::max<long long>(s->peak_job, (long long)nodes[k]);
   if (c->ctl_host->error) {
     // a device wait ran out or an epoch's outputs did not fit: finish_launch
     // dropped the frontier, so every running job ends with that status and
@@ -2044,31 +2110,8 @@ extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int
       s->slot_job[k].reset();
       after -= (long long)nodes[k];
     }
-    // bottom to top: the jobs that stay in the usual order, then the ones
-    // leaving, which are then copied out from above the new top
-    int lay[kMaxJobs], m = 0;
-    for (int i = first; i < n; ++i) lay[m++] = order[i];
-    for (int i = first - 1; i >= 0; --i) lay[m++] = order[i];
     int rc;
-    if ((rc = regroup(s, lay, m, nodes))) return rc;
-    long long pos = after;
-    for (int i = first - 1; i >= 0; --i) {
-      const int k = order[i];
-      if (s->slot_job[k]) {
-        std::unique_ptr<ServeJob> j = std::move(s->slot_job[k]);
-        j->saved.resize((size_t)nodes[k]);
-        CK(d2h(c, j->saved.data(), c->stack + pos, sizeof(Node) * (size_t)nodes[k]));
-        memcpy(j->saved_cnt, cnt + k * kJobCounters, sizeof j->saved_cnt);
-        j->swapped = true;
-        j->reserve = std::max<long long>(j->reserve, 2 * (long long)nodes[k]);
-        j->slot = -1;
-        s->queue.push_front(std::move(j));
-        ++s->evictions;
-      }
-      pos += (long long)nodes[k];
-    }
-    CK(cudaStreamSynchronize(c->stream));
-    if ((rc = set_top(s, after))) return rc;
+    if ((rc = swap_out(s, order, n, first, nodes, cnt, after))) return rc;
     n = 0;  // the frontier is in order already
   }
   if (n > 1 && complete) s->reorder = true;
@@ -2104,10 +2147,13 @@ extern "C" int e13_serve_survivors(e13_serve *s, int64_t id, e13_survivor *out, 
   return rc;
 }
 
-extern "C" int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs, int64_t *swapped_out) {
+extern "C" int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs, int64_t *swapped_out,
+                               int64_t *peak_nodes, int64_t *peak_job_nodes) {
   if (!s) return E13_ERR_ARG;
   if (device_ms) *device_ms = s->device_ms;
   if (epochs) *epochs = s->epochs;
   if (swapped_out) *swapped_out = s->evictions;
+  if (peak_nodes) *peak_nodes = s->peak_top;
+  if (peak_job_nodes) *peak_job_nodes = s->peak_job;
   return E13_OK;
 }

@@ -149,7 +149,7 @@ def lib():
                                         P(ctypes.c_size_t)]
         L.e13_estimate.argtypes = [ctypes.c_void_p, P(Job), ctypes.c_int64, ctypes.c_uint64, P(EstimateOut),
                                    P(ctypes.c_double)]
-        L.e13_autotune.argtypes = [ctypes.c_void_p, P(Job), P(Tuning), P(Tuning), P(ctypes.c_double)]
+        L.e13_autotune.argtypes = [ctypes.c_void_p, P(Job), ctypes.c_int32, P(Tuning), P(Tuning), P(ctypes.c_double)]
         L.e13_serve_create.argtypes = [ctypes.c_void_p, P(Tuning), ctypes.c_int64, P(ctypes.c_void_p)]
         L.e13_serve_destroy.argtypes = [ctypes.c_void_p]
         L.e13_serve_destroy.restype = None
@@ -161,7 +161,9 @@ def lib():
         L.e13_serve_pending.argtypes = [ctypes.c_void_p]
         L.e13_serve_pending.restype = ctypes.c_int64
         L.e13_serve_survivors.argtypes = [ctypes.c_void_p, ctypes.c_int64, P(Survivor), I, P(I)]
-        L.e13_serve_stats.argtypes = [ctypes.c_void_p, P(ctypes.c_double), P(ctypes.c_int64), P(ctypes.c_int64)]
+        L.e13_serve_stats.argtypes = [ctypes.c_void_p, P(ctypes.c_double), P(ctypes.c_int64), P(ctypes.c_int64),
+                                      P(ctypes.c_int64), P(ctypes.c_int64)]
+        L.e13_serve_preempt.argtypes = [ctypes.c_void_p, ctypes.c_int64]
         L.e13_run_full.argtypes = [ctypes.c_void_p, P(ctypes.c_int32), I, I, P(ctypes.c_int64)]
         L.e13_check.argtypes = [ctypes.c_void_p, P(CheckIn), I, I, I, P(CheckOut)]
         L.e13_check_noalloc.argtypes = [I, P(CheckIn), I, I, I, P(CheckOut)]
@@ -180,7 +182,7 @@ EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine
             "e13_format_recheck", "e13_format_deep", "e13_check_crafted", "e13_raw_run", "e13_autotune", "e13_check_noalloc",
             "e13_serve_create", "e13_serve_destroy", "e13_serve_clock", "e13_serve_submit", "e13_serve_step",
             "e13_serve_pending", "e13_serve_survivors", "e13_serve_stats", "e13_resolve_tuning",
-            "e13_selftest_pool_wait", "e13_serve_submit_shard"]
+            "e13_selftest_pool_wait", "e13_serve_submit_shard", "e13_serve_preempt"]
 
 
 def keys():
@@ -480,14 +482,25 @@ class Server:
         """(device ms of all epochs, epochs)."""
         ms = ctypes.c_double()
         ep = ctypes.c_int64()
-        lib().e13_serve_stats(self.h, ctypes.byref(ms), ctypes.byref(ep), None)
+        lib().e13_serve_stats(self.h, ctypes.byref(ms), ctypes.byref(ep), None, None, None)
         return ms.value, ep.value
 
     def swapped_out(self) -> int:
         """Times a job was swapped out to host memory to make room."""
         n = ctypes.c_int64()
-        lib().e13_serve_stats(self.h, None, None, ctypes.byref(n))
+        lib().e13_serve_stats(self.h, None, None, ctypes.byref(n), None, None)
         return n.value
+
+    def peaks(self):
+        """(largest frontier after an epoch, largest share of it one job held), in nodes."""
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        lib().e13_serve_stats(self.h, None, None, None, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def preempt(self, job_id: int):
+        r = lib().e13_serve_preempt(self.h, job_id)
+        if r:
+            raise E13Error(r, "e13_serve_preempt")
 
     def run_all(self, jobs, arrivals=None, shard=0, nshards=1):
         """Submits jobs (with optional arrival times; with nshards > 1 this

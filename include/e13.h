@@ -319,9 +319,19 @@ int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int *ndone);
 int64_t e13_serve_pending(const e13_serve *s);
 /* Survivors of a finished job (once; *n = all it found). */
 int e13_serve_survivors(e13_serve *s, int64_t id, e13_survivor *out, int cap, int *n);
-/* CUDA-event time of all epochs, their number, and how many times a job was
-   swapped out to host memory to make room (each pointer may be NULL). */
-int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs, int64_t *swapped_out);
+/* CUDA-event time of all epochs, their number, how many times a job was
+   swapped out to host memory, the largest frontier after an epoch and the
+   largest share of it one job held, in nodes (each pointer may be NULL). */
+int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs, int64_t *swapped_out,
+                    int64_t *peak_nodes, int64_t *peak_job_nodes);
+/* Preempts a running job between steps: its frontier nodes and counters go
+   to host memory and it returns to the head of the queue, to be resumed where
+   it stopped when it is admitted again (its counts stay exact).  The same swap
+   the session makes by itself when the frontier runs out of room; a caller
+   uses it to make room for more urgent jobs.  E13_OK also for a job that is
+   queued; E13_ERR_ARG for an unknown or finished id.  No counterpart in the
+   reference. */
+int e13_serve_preempt(e13_serve *s, int64_t id);
 
 /* Autotuner (no counterpart in the reference, which has one fixed GPU
    launch shape, src/e13gpu.py:342-346, and a fixed serial split depth,

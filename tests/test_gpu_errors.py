@@ -33,7 +33,8 @@ def test_frontier_overflow_is_reported_and_the_context_recovers(searches, kernel
     e = searches["local_edits_f3"]
     job = make_job(e, 11)  # 1.4e7 leaves: its frontier outgrows 2,000 nodes at once
     with pytest.raises(E.E13Error) as ei:
-        ctx().search(job, E.tuning(kernel=KERNELS[kernel], stack_nodes=2000))
+        # 1 ms epochs: the persistent kernel dumps its lanes and warp stacks onto the frontier at once
+        ctx().search(job, E.tuning(kernel=KERNELS[kernel], stack_nodes=2000, epoch_us=1000))
     assert ei.value.code == -6  # E13_ERR_OVERFLOW
     _golden_f2_x8(searches)
     c, _ = ctx().search(job, E.tuning(kernel=KERNELS[kernel]))

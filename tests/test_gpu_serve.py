@@ -76,25 +76,61 @@ def test_big_and_small_jobs_interleave(searches):
     assert sorted(E.survivor_line(jobs[-1], s) for s in surv) == golden_lines(searches["counter_sym"])
 
 
-def test_swap_out_keeps_results(searches):
-    """A frontier capacity too small for the jobs running together: after an
-    epoch the jobs with the most live nodes are swapped out to host memory and
-    resumed later.  Every job's counts and survivors still equal the
-    reference's; at least one swap happened."""
-    mix = [(searches["local_edits_f3"], X) for X in range(14)] + [(searches["counter_sym"], 13)]
-    jobs = [make_job(e, X) for e, X in mix]
-    # small launch shape: one epoch's outputs need 2 * 1184 * 48 + 65536 nodes of room
-    tune = E.tuning(block=256, warp_stack=16, stack_nodes=2 * 1184 * 48 + 65536 + 60000, epoch_us=5000)
-    with E.Server(ctx(), tune) as srv:
-        got = srv.run_all(jobs)
-        swaps = srv.swapped_out()
-    assert swaps > 0
+def _swap_mix(searches):
+    return [(searches["local_edits_f3"], X) for X in range(14)] + [(searches["counter_sym"], 13)]
+
+
+def _check_mix(searches, mix, jobs, got):
     for i, (e, X) in enumerate(mix):
         res, surv = got[i]
         assert res.status == 0, (X, res.status)
         check_entry(dict(e, expect=[_expect(e, X)]), [res.counts.as_dict()])
     res, surv = got[len(mix) - 1]
     assert sorted(E.survivor_line(jobs[-1], s) for s in surv) == golden_lines(searches["counter_sym"])
+
+
+def test_preempted_jobs_resume_exactly(searches):
+    """Jobs preempted between steps (e13_serve_preempt: frontier nodes and
+    counters to host memory, back to the head of the queue) resume where they
+    stopped: every job's counts and survivors equal the reference's."""
+    mix = _swap_mix(searches)
+    jobs = [make_job(e, X) for e, X in mix]
+    with E.Server(ctx(), E.tuning(epoch_us=2000)) as srv:
+        for i, job in enumerate(jobs):
+            srv.submit(job, i)
+        got, steps = {}, 0
+        while srv.pending():
+            for r in srv.step():
+                got[r.id] = (r, srv.survivors(r.id))
+            steps += 1
+            if steps % 3 == 0:  # preempt the lowest-numbered unfinished job (a no-op while it is queued)
+                k = min(i for i in range(len(jobs)) if i not in got)
+                srv.preempt(k)
+        swaps = srv.swapped_out()
+    assert swaps > 0
+    _check_mix(searches, mix, jobs, got)
+
+
+def test_swap_out_when_the_frontier_runs_out_of_room(searches):
+    """A frontier capacity between one job's largest frontier and the jobs'
+    largest frontier together: after an epoch the jobs with the most live
+    nodes are swapped out by the session itself and resumed later; results
+    still equal the reference's."""
+    mix = _swap_mix(searches)
+    jobs = [make_job(e, X) for e, X in mix]
+    block, ws = 256, 16
+    out_nodes = 2 * (148 * block // 32) * (32 + ws) + 65536  # one epoch's output room at this launch shape
+    tune = E.tuning(block=block, warp_stack=ws, epoch_us=2000)
+    with E.Server(ctx(), tune, reserve_nodes=64) as srv:  # small reservations: every job is admitted at once
+        srv.run_all(jobs)
+        peak, peak_job = srv.peaks()
+    assert peak > peak_job
+    tune.stack_nodes = out_nodes + (peak + 2 * peak_job) // 3
+    with E.Server(ctx(), tune, reserve_nodes=64) as srv:
+        got = srv.run_all(jobs)
+        swaps = srv.swapped_out()
+    assert swaps > 0, (peak, peak_job)
+    _check_mix(searches, mix, jobs, got)
 
 
 def test_admission_reserves_by_estimate(searches):
