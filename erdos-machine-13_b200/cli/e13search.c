@@ -14,7 +14,7 @@
    sample of the same estimator: they equal the reference probe for probe, not
    line for line.  Environment: E13_DEVICE (CUDA device, default 0), E13_KERNEL
    (persistent | plain), E13_AUTOTUNE=N (tune the persistent kernel on 1/N of
-   the first job before searching; see maybe_autotune).  There is no CPU path:
+   the command's jobs before searching; see maybe_autotune).  There is no CPU path:
    without a GPU it exits 1.
 
    free / freesym keep checkpoints as src/e13gpu.py:349-409 does: E13_CKPT
@@ -45,22 +45,20 @@ static e13_ctx *open_ctx(void) {
   return ctx;
 }
 
-/* E13_AUTOTUNE=N (N >= 1): before the first search, tune the persistent
-   kernel on shard 0 of N of that search's job (N = 1: the whole job) and use
-   the result for every search of the command. */
-static void maybe_autotune(e13_ctx *ctx, const e13_job *job, e13_tuning *tu) {
-  static int done = 0;
+/* E13_AUTOTUNE=N (N >= 1): before searching, tune the persistent kernel on
+   shard 0 of N of each of the command's n jobs, run together (N = 1: the whole
+   jobs), and use the result for every search of the command. */
+static void maybe_autotune(e13_ctx *ctx, const e13_job *jobs, int n, e13_tuning *tu) {
   const char *a = getenv("E13_AUTOTUNE");
-  if (done || !a || atoi(a) < 1 || tu->kernel != E13_KERNEL_PERSISTENT) return;
-  done = 1;
+  if (!a || atoi(a) < 1 || n < 1 || tu->kernel != E13_KERNEL_PERSISTENT) return;
   e13_tuning best;
   double ms = 0;
-  int rc = e13_autotune(ctx, job, atoi(a), tu, &best, &ms);
+  int rc = e13_autotune_jobs(ctx, jobs, n, atoi(a), tu, &best, &ms);
   if (rc) {
     fprintf(stderr, "autotune failed (error %d): default tuning kept\n", rc);
     return;
   }
-  fprintf(stderr, "autotune X=%d proxy=1/%d: block=%d slice=%d warp_stack=%d pool_low_pct=%d (%.1f ms)\n", job->X,
+  fprintf(stderr, "autotune jobs=%d proxy=1/%d: block=%d slice=%d warp_stack=%d pool_low_pct=%d (%.1f ms)\n", n,
           atoi(a), best.block, best.slice, best.warp_stack, best.pool_low_pct, ms);
   *tu = best;
 }
@@ -170,21 +168,31 @@ int main(int argc, char **argv) {
     if (argc < 5) return 1;
     int fmax = atoi(argv[3]);
     e13_ctx *ctx = open_ctx();
-    for (int i = 4; i < argc; i++) {
-      e13_job job;
-      int X = atoi(argv[i]);
-      int rc = e13_setup(base, nq0, X, fmax, NULL, -1, -1, &job);
-      if (rc == E13_ERR_FMAX) {
-        fprintf(stderr, "X=%d forced=%d > fmax\n", X, job.nforced);
+    /* every job set up first, so the autotuner sees them all; the reference's
+       messages then come in argument order, between the searches */
+    const int na = argc - 4;
+    e13_job *jobs = (e13_job *)malloc(sizeof(e13_job) * (size_t)na);
+    e13_job *runnable = (e13_job *)malloc(sizeof(e13_job) * (size_t)na);
+    int *st = (int *)malloc(sizeof(int) * (size_t)na), n = 0;
+    for (int i = 0; i < na; i++) {
+      st[i] = e13_setup(base, nq0, atoi(argv[4 + i]), fmax, NULL, -1, -1, &jobs[i]);
+      if (st[i] == 0) runnable[n++] = jobs[i];
+    }
+    maybe_autotune(ctx, runnable, n, &tu);
+    for (int i = 0; i < na; i++) {
+      if (st[i] == E13_ERR_FMAX) {
+        fprintf(stderr, "X=%d forced=%d > fmax\n", jobs[i].X, jobs[i].nforced);
         continue;
       }
-      if (rc) {
-        fprintf(stderr, "X=%d: setup error %d\n", X, rc);
+      if (st[i]) {
+        fprintf(stderr, "X=%d: setup error %d\n", jobs[i].X, st[i]);
         return 1;
       }
-      maybe_autotune(ctx, &job, &tu);
-      if (run_one(ctx, &job, &tu, NULL)) return 1;
+      if (run_one(ctx, &jobs[i], &tu, NULL)) return 1;
     }
+    free(jobs);
+    free(runnable);
+    free(st);
     e13_ctx_destroy(ctx);
     return 0;
   }
@@ -225,7 +233,7 @@ int main(int argc, char **argv) {
     const char *cksec = getenv("E13_CKPT_SEC");
     e13_checkpoint ck = {ckpath, config, cksec ? atof(cksec) : 1800.0, 0.0};
     e13_ctx *ctx = open_ctx();
-    maybe_autotune(ctx, &job, &tu);
+    maybe_autotune(ctx, &job, 1, &tu);
     rc = run_one(ctx, &job, &tu, (ckpath && ckpath[0]) ? &ck : NULL);
     e13_ctx_destroy(ctx);
     return rc == E13_STOPPED ? 3 : (rc ? 1 : 0);

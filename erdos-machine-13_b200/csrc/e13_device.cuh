@@ -83,6 +83,7 @@ struct Ctl {
   unsigned long long nsurv;      // survivors found (records kept: min(nsurv, cap))
   int dump;                      // persistent: end the epoch now
   int busy;                      // persistent: warps holding work or claiming it
+  int idle;                      // persistent: warps waiting for work (starved)
   int error;                     // kErr* bits
   int launches;
   // utilisation counters: warp rounds, running lanes summed over rounds,

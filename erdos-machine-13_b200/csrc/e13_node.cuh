@@ -12,10 +12,9 @@
 namespace e13dev {
 
 __device__ __forceinline__ void lane_load(Lane &L, const Node *N, u32 *tcol, u32 *rcol, int stride, int nq) {
-  // clear what the previous machine of this lane may have written
-  int lo, hi;
-  tape_extent(L.t, lo, hi);
-  for (int w = lo; w <= hi; ++w) tcol[w * stride] = 0;
+  // the words the previous machine of this lane may have written
+  int lo_old, hi_old;
+  tape_extent(L.t, lo_old, hi_old);
   L.p = N->p;
   L.st = N->st;
   L.t = N->t;
@@ -42,8 +41,12 @@ __device__ __forceinline__ void lane_load(Lane &L, const Node *N, u32 *tcol, u32
     rcol[(4 * k + 2) * stride] = v.z;
     rcol[(4 * k + 3) * stride] = v.w;
   }
+  // one pass over both extents: the new machine's words are copied, the old
+  // machine's other words cleared (siblings of one fork share most words)
+  int lo, hi;
   tape_extent(L.t, lo, hi);
-  for (int w = lo; w <= hi; ++w) tcol[w * stride] = N->tape[w];
+  const int a = lo < lo_old ? lo : lo_old, b = hi > hi_old ? hi : hi_old;
+  for (int w = a; w <= b; ++w) tcol[w * stride] = (w >= lo && w <= hi) ? N->tape[w] : 0u;
 }
 
 __device__ __forceinline__ void lane_store(const Lane &L, Node *N, const u32 *tcol, const u32 *rcol, int stride,

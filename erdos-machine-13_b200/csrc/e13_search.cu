@@ -50,6 +50,7 @@ constexpr int kKeySmemBytes = (kTapeCells + 64) * 8;
 constexpr long long kPoolNodes = 1LL << 18;  // donation pool: 256 Ki nodes (80 MiB)
 constexpr long long kWholeFrontier = 1LL << 62;  // persistent batch when e13_tuning::batch is 0
 constexpr long long kPoolWaitNs = 200000000;     // 200 ms: a donor publishes a claimed slot within microseconds
+constexpr long long kMinEpochNs = 200000;        // 200 us: the shortest epoch a starvation dump may end
 
 // steps a lane gets between warp-level refill rounds is Params::slice
 
@@ -61,6 +62,7 @@ struct Params {
   long long out_cap, out_soft, surv_cap, pool_cap;
   long long epoch_ns;
   long long wait_ns;         // persistent: limit of the wait for a claimed pool slot's data
+  long long min_epoch_ns;    // persistent: an epoch may end early for starvation only after this long
   Node *stack, *out, *wstack, *pool;
   int *pool_ready;
   SurvRec *surv;
@@ -131,7 +133,7 @@ static __device__ __noinline__ void record_survivor(Ctl *ctl, SurvRec *surv, lon
   r->job = job;
 }
 
-enum { kStRun = 0, kStIdle = 1, kStFork = 2, kStCap = 3 };
+enum { kStRun = 0, kStIdle = 1, kStFork = 2, kStCap = 3, kStDead = 4, kStSurv = 5 };
 
 __device__ __forceinline__ int wrap(int s, int d) { return s >= d ? s - d : s; }
 
@@ -178,13 +180,18 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   L.tseg = 0;
   // leaves and steps of this lane's current job, added to the block's per-job
   // counters only when the lane changes job and at the end (no atomics per leaf)
-  u32 acc_leaves = 0, acc_steps = 0;
+  // (deaths at stages 0 and 1, 97 % of all leaves, are counted per lane too:
+  // two 16-bit halves of acc_d01, flushed before either can overflow)
+  u32 acc_leaves = 0, acc_steps = 0, acc_d01 = 0;
   auto flush_counts = [&]() {
     if (acc_leaves | acc_steps) {
       atomicAdd(&s_jc[L.job][0], (unsigned long long)acc_leaves);
       atomicAdd(&s_jc[L.job][1], (unsigned long long)acc_steps);
+      if (acc_d01 & 0xFFFFu) atomicAdd(&s_jc[L.job][2], (unsigned long long)(acc_d01 & 0xFFFFu));
+      if (acc_d01 >> 16) atomicAdd(&s_jc[L.job][3], (unsigned long long)(acc_d01 >> 16));
       acc_leaves = 0;
       acc_steps = 0;
+      acc_d01 = 0;
     }
   };
   int status = kStIdle;
@@ -201,6 +208,8 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   bool input_done = false;
   bool busy = false;           // persistent: counted in ctl->busy
   bool top_dirty = false;      // persistent: the stack top lives only in the shared copy (its HBM slot is stale)
+  bool counted_idle = false;   // persistent, lane 0: this warp is counted in ctl->idle
+  const int nwarps_all = (int)(((long long)gridDim.x * stride) >> 5);
   int rounds = 0;              // slices run: a warp dumps only after one (progress every epoch)
   unsigned backoff = 256;
   unsigned long long st_lane_rounds = 0, st_polls = 0;
@@ -371,6 +380,10 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
             }
           }
           if (!src) break;
+          if (PERSIST && counted_idle && lane == 0) {
+            atomicSub(&ctl->idle, 1);
+            counted_idle = false;
+          }
           if (PERSIST) {
             wbot = 0;
             if (lane < kNodeChunks) {
@@ -447,6 +460,21 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
         }
         done = __shfl_sync(kFull, done, 0);
         if (done) break;
+        // starving.  Work spreads inside an epoch only through donated nodes,
+        // which a few deep warps hand out one at a time: a job whose subtrees
+        // are shallow would run on a few warps for a long time.  When more
+        // than half of the warps wait for work, end the epoch (after a
+        // shortest length): the dump puts every warp's stack on the frontier
+        // and the next epoch deals it out over all warps.
+        if (lane == 0) {
+          if (!counted_idle) {
+            atomicAdd(&ctl->idle, 1);
+            counted_idle = true;
+          } else if (backoff >= 1024 && globaltimer() - t_begin > (unsigned long long)P.min_epoch_ns &&
+                     2 * *((volatile int *)&ctl->idle) > nwarps_all) {
+            *((volatile int *)&ctl->dump) = 1;
+          }
+        }
         ++st_polls;
         __nanosleep(backoff);
         backoff = backoff < 8192 ? 2 * backoff : 8192;
@@ -505,7 +533,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
       }
     }
 
-    // ---- (D) run a slice: every running lane takes one action per iteration
+    // ---- (D) run a slice: every running lane takes up to two actions per iteration
     ++rounds;
     {
       const unsigned rm = __ballot_sync(kFull, status == kStRun);
@@ -516,7 +544,10 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
           if (status == kStRun) {
             int cell = 0;
             u32 e = 0;
+            // two actions per iteration: the loop control and the event
+            // dispatch below are paid once for both
             int ev = lane_act(L, tcol, rcol, keyb, keyc, stride, cell, e);
+            if (!ev) ev = lane_act(L, tcol, rcol, keyb, keyc, stride, cell, e);
             if (ev == kEvCell) {
               if (e == kEntHalt) {
                 ev = kEvDead;
@@ -538,22 +569,34 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
                 ev = ((e & 0x7Fu) == kEntHalt) ? kEvDead : 0;
               }
             }
-            if (ev) {
-              // a leaf
-              acc_steps += (u32)(L.t - L.tseg);
-              L.tseg = L.t;
-              ++acc_leaves;
-              if (acc_steps >= 0x80000000u) flush_counts();
-              if (ev == kEvDead) atomicAdd(&s_jc[L.job][2 + L.stage], 1ull);
-              else record_survivor(P.ctl, P.surv, P.surv_cap, L.st0, L.p0, L.flags, L.t, L.job, tcol, rcol, stride,
-                                   PERSIST);
-              status = kStIdle;
-            }
+            // a leaf: counted by the warp after the slice, all its leaves in
+            // one converged pass (the lane would wait for the next round anyway)
+            if (ev) status = (ev == kEvDead) ? kStDead : kStSurv;
           }
           // every lane comes here each iteration (the loop bounds are
-          // warp-uniform): rejoin the lanes that took rare branches so the next
-          // action issues once for the whole warp
-          __syncwarp();
+          // warp-uniform): the lanes that took rare branches rejoin at the end
+          // of the if-blocks above, so the next action issues once for the
+          // whole warp
+        }
+        if (__any_sync(kFull, status >= kStDead)) {
+          if (status >= kStDead) {
+            acc_steps += (u32)(L.t - L.tseg);
+            L.tseg = L.t;
+            ++acc_leaves;
+            if (acc_steps >= 0x80000000u) flush_counts();
+            if (status == kStDead) {
+              if (L.stage <= 1) {
+                acc_d01 += L.stage ? 0x10000u : 1u;
+                if (acc_d01 & 0x80008000u) flush_counts();
+              } else {
+                atomicAdd(&s_jc[L.job][2 + L.stage], 1ull);
+              }
+            } else {
+              record_survivor(P.ctl, P.surv, P.surv_cap, L.st0, L.p0, L.flags, L.t, L.job, tcol, rcol, stride,
+                              PERSIST);
+            }
+            status = kStIdle;
+          }
         }
         if (!PERSIST && status == kStRun && L.t - L.tseg >= P.step_cap) {
           acc_steps += (u32)(L.t - L.tseg);
@@ -680,6 +723,7 @@ __global__ void finish_launch(Ctl *ctl, long long cap, long long batch_max, long
   ctl->nout = 0;
   ctl->dump = 0;
   ctl->busy = 0;
+  ctl->idle = 0;
   ctl->pool_head = 0;
   ctl->pool_tail = 0;
   ctl->launches += 1;
@@ -914,6 +958,7 @@ static Params make_params(const e13_ctx *c, const e13_tuning &tu, int nq, long l
   P.surv_cap = c->surv_cap;
   P.epoch_ns = (long long)tu.epoch_us * 1000LL;
   P.wait_ns = kPoolWaitNs;
+  P.min_epoch_ns = kMinEpochNs;
   P.stack = c->stack;
   P.out = c->out;
   P.wstack = c->wstack;
@@ -1154,6 +1199,8 @@ static ShardKey shard_key(const Node &n) {
 
 constexpr long long kSplitPerShard = 512;  // frontier nodes per shard before the deal
 constexpr int kSplitLevels = 24;           // most plain launches of the split
+constexpr int kSplitSlice = 24;            // the split's slice and step cap (fixed: they shape the frontier)
+constexpr int kSplitStepCap = 20000;
 
 // One share of a search split over nshards (the reference's SPLIT frontier,
 // src/e13search.c:222-235, built for the device): the plain kernel expands the
@@ -1164,7 +1211,11 @@ constexpr int kSplitLevels = 24;           // most plain launches of the split
 // survivors, with their read masks) counts in shard 0 only: *cnt and *recs
 // are zero / empty for the other shards.  Runs on buffers of its own (freed
 // before it returns), so a serve session's frontier is left alone; `slot` is
-// the job slot written into the nodes.
+// the job slot written into the nodes.  The expansion runs with a fixed
+// slice, step cap and run skip: a lane is requeued at the first slice end
+// past the step cap, so those settings shape the frontier, and with them fixed
+// every shard's content depends on the job alone, whatever tuning the caller's
+// search then uses (the autotuner compares shard 0 across tunings).
 static int split_share(e13_ctx *c, const e13_job *job, const e13_tuning &tu, int shard, int nshards, int slot,
                        std::vector<Node> &mine, unsigned long long cnt[kJobCounters], std::vector<SurvRec> &recs,
                        long long *launches) {
@@ -1192,7 +1243,7 @@ static int split_share(e13_ctx *c, const e13_job *job, const e13_tuning &tu, int
   jp[slot].sym_lo = job->sym_lo;
   jp[slot].sym_hi = job->sym_hi;
   Node root;
-  build_root(job, slot, &root, tu.run_skip != 0, true);
+  build_root(job, slot, &root, true, true);
   Ctl h;
   memset(&h, 0, sizeof h);
   h.top = 1;
@@ -1210,6 +1261,9 @@ static int split_share(e13_ctx *c, const e13_job *job, const e13_tuning &tu, int
       !fail(cudaMemsetAsync(jobcnt, 0, sizeof(unsigned long long) * kMaxJobs * kJobCounters, c->stream), "memset")) {
     e13_tuning t = tu;
     t.kernel = E13_KERNEL_PLAIN;
+    t.slice = kSplitSlice;
+    t.step_cap = kSplitStepCap;
+    t.run_skip = 1;
     Params S = make_params(c, t, job->nq, nwarps, nwarps * 32);
     S.jobs = jobs;
     S.jobcnt = jobcnt;
@@ -1580,41 +1634,65 @@ extern "C" int e13_selftest_pool_wait(e13_ctx *c, int32_t wait_us) {
 // ------------------------------------------------------------------------
 // autotuner
 
-extern "C" int e13_autotune(e13_ctx *c, const e13_job *job, int32_t proxy_shards, const e13_tuning *start,
-                            e13_tuning *best, double *best_ms) {
-  if (!c || !job || !best || proxy_shards < 0 || proxy_shards > 4096) return E13_ERR_ARG;
+// The autotuner times candidates through serve sessions (defined below).
+extern "C" int e13_serve_create(e13_ctx *ctx, const e13_tuning *tuning, int64_t reserve_nodes, e13_serve **out);
+extern "C" void e13_serve_destroy(e13_serve *s);
+extern "C" int e13_serve_submit(e13_serve *s, const e13_job *job, int64_t id, double t_submit);
+extern "C" int e13_serve_submit_shard(e13_serve *s, const e13_job *job, int64_t id, double t_submit, int shard,
+                                      int nshards);
+extern "C" int e13_serve_step(e13_serve *s, e13_serve_result *done, int cap, int *ndone);
+extern "C" int64_t e13_serve_pending(const e13_serve *s);
+extern "C" int e13_serve_stats(const e13_serve *s, double *device_ms, int64_t *epochs, int64_t *swapped_out,
+                               int64_t *peak_nodes, int64_t *peak_job_nodes);
+
+extern "C" int e13_autotune_jobs(e13_ctx *c, const e13_job *jobs, int n, int32_t proxy_shards,
+                                 const e13_tuning *start, e13_tuning *best, double *best_ms) {
+  if (!c || !jobs || n < 1 || n > 4096 || !best || proxy_shards < 0 || proxy_shards > 4096) return E13_ERR_ARG;
   e13_tuning cur;
   if (e13_resolve_tuning(start, 0, &cur) != E13_OK) return E13_ERR_ARG;
   cur.kernel = E13_KERNEL_PERSISTENT;
   const int nsh = proxy_shards > 1 ? proxy_shards : 1;
-  e13_counts ref_counts, got;
-  int ns = 0;
-  std::vector<e13_survivor> surv(4096);
-  // the proxy: shard 0 of the job's own subtrees (e13_search_shard), so the
-  // tuning is timed on the job's own mix of machines at a fraction of its cost
-  auto run = [&](const e13_tuning &t, e13_counts *out, double *ms) -> int {
-    const int rc = e13_search_shard(c, job, &t, 0, nsh, out, surv.data(), (int)surv.size(), &ns);
-    if (rc && rc != E13_ERR_SURV_CAP) return rc;
-    *ms = c->stats.device_ms;
-    return E13_OK;
+  // a candidate: shard 0 of nsh of every job, all in one serve session (the
+  // way a workload of several jobs runs), timed over its epochs; every job's
+  // counts are kept to check that the tuning changes no result
+  auto run = [&](const e13_tuning &t, std::vector<e13_counts> &out, double *ms) -> int {
+    e13_serve *s = nullptr;
+    int rc = e13_serve_create(c, &t, 0, &s);
+    if (rc) return rc;
+    out.assign((size_t)n, e13_counts());
+    for (int i = 0; i < n && !rc; ++i)
+      rc = nsh > 1 ? e13_serve_submit_shard(s, &jobs[i], i, 0.0, 0, nsh) : e13_serve_submit(s, &jobs[i], i, 0.0);
+    e13_serve_result done[kMaxJobs];
+    while (!rc && e13_serve_pending(s) > 0) {
+      int nd = 0;
+      rc = e13_serve_step(s, done, kMaxJobs, &nd);
+      for (int k = 0; k < nd && !rc; ++k) {
+        if (done[k].status != E13_OK && done[k].status != E13_ERR_SURV_CAP) rc = done[k].status;
+        else out[(size_t)done[k].id] = done[k].counts;
+      }
+    }
+    if (!rc) e13_serve_stats(s, ms, nullptr, nullptr, nullptr, nullptr);
+    e13_serve_destroy(s);
+    return rc;
   };
+  std::vector<e13_counts> ref, got;
   double cur_ms = 0;
-  int rc = run(cur, &ref_counts, &cur_ms);  // warms the buffers up
+  int rc = run(cur, ref, &cur_ms);  // warms the buffers up
   if (rc) return rc;
-  if ((rc = run(cur, &got, &cur_ms))) return rc;
-  if (memcmp(&got, &ref_counts, sizeof got) != 0) return E13_ERR_CUDA;
+  if ((rc = run(cur, got, &cur_ms))) return rc;
+  if (memcmp(got.data(), ref.data(), sizeof(e13_counts) * (size_t)n) != 0) return E13_ERR_CUDA;
   struct Axis {
     int32_t e13_tuning::*field;
     int vals[5];
     int n;
   };
-  // block: lanes per CTA (one CTA per SM); slice: actions between a warp's
-  // refill rounds; warp_stack: the depth of subtree a warp keeps to itself
-  // before it spills or donates; pool_low_pct: the threshold below which warps
-  // with deep stacks fork work off to idle warps
+  // block: lanes per CTA (one CTA per SM); slice: iterations between a
+  // warp's refill rounds; warp_stack: the depth of subtree a warp keeps to
+  // itself before it spills or donates; pool_low_pct: the threshold below
+  // which warps with deep stacks fork work off to idle warps
   const Axis axes[] = {
       {&e13_tuning::block, {512, 640, 768, 0, 0}, 3},
-      {&e13_tuning::slice, {12, 16, 24, 32, 48}, 5},
+      {&e13_tuning::slice, {6, 8, 12, 16, 24}, 5},
       {&e13_tuning::warp_stack, {64, 128, 256, 512, 0}, 4},
       {&e13_tuning::pool_low_pct, {2, 5, 12, 25, 0}, 4},
   };
@@ -1626,9 +1704,10 @@ extern "C" int e13_autotune(e13_ctx *c, const e13_job *job, int32_t proxy_shards
       e13_tuning t = cur;
       t.*(ax.field) = ax.vals[i];
       double ms = 0;
-      if ((rc = run(t, &got, &ms))) return rc;
-      if (memcmp(&got, &ref_counts, sizeof got) != 0) return E13_ERR_CUDA;  // results must not depend on tuning
-      if (ms < axis_ms * 0.98) {  // a 2 % margin keeps timing noise from moving the choice
+      if ((rc = run(t, got, &ms))) return rc;
+      if (memcmp(got.data(), ref.data(), sizeof(e13_counts) * (size_t)n) != 0)
+        return E13_ERR_CUDA;  // results must not depend on tuning
+      if (ms < axis_ms * 0.97) {  // a 3 % margin keeps timing noise from moving the choice
         axis_ms = ms;
         axis_best = t;
       }
@@ -1639,6 +1718,11 @@ extern "C" int e13_autotune(e13_ctx *c, const e13_job *job, int32_t proxy_shards
   *best = cur;
   if (best_ms) *best_ms = cur_ms;
   return E13_OK;
+}
+
+extern "C" int e13_autotune(e13_ctx *c, const e13_job *job, int32_t proxy_shards, const e13_tuning *start,
+                            e13_tuning *best, double *best_ms) {
+  return e13_autotune_jobs(c, job, 1, proxy_shards, start, best, best_ms);
 }
 
 // ------------------------------------------------------------------------

@@ -150,6 +150,8 @@ def lib():
         L.e13_estimate.argtypes = [ctypes.c_void_p, P(Job), ctypes.c_int64, ctypes.c_uint64, P(EstimateOut),
                                    P(ctypes.c_double)]
         L.e13_autotune.argtypes = [ctypes.c_void_p, P(Job), ctypes.c_int32, P(Tuning), P(Tuning), P(ctypes.c_double)]
+        L.e13_autotune_jobs.argtypes = [ctypes.c_void_p, P(Job), I, ctypes.c_int32, P(Tuning), P(Tuning),
+                                        P(ctypes.c_double)]
         L.e13_serve_create.argtypes = [ctypes.c_void_p, P(Tuning), ctypes.c_int64, P(ctypes.c_void_p)]
         L.e13_serve_destroy.argtypes = [ctypes.c_void_p]
         L.e13_serve_destroy.restype = None
@@ -182,7 +184,7 @@ EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine
             "e13_format_recheck", "e13_format_deep", "e13_check_crafted", "e13_raw_run", "e13_autotune", "e13_check_noalloc",
             "e13_serve_create", "e13_serve_destroy", "e13_serve_clock", "e13_serve_submit", "e13_serve_step",
             "e13_serve_pending", "e13_serve_survivors", "e13_serve_stats", "e13_resolve_tuning",
-            "e13_selftest_pool_wait", "e13_serve_submit_shard", "e13_serve_preempt"]
+            "e13_selftest_pool_wait", "e13_serve_submit_shard", "e13_serve_preempt", "e13_autotune_jobs"]
 
 
 def keys():
@@ -341,6 +343,18 @@ class Context:
                                ctypes.byref(best), ctypes.byref(ms))
         if r:
             raise E13Error(r, "e13_autotune")
+        return best, ms.value
+
+    def autotune_jobs(self, jobs, start: Tuning | None = None, proxy_shards: int = 1):
+        """Coordinate-descent tuning timed on shard 0 of proxy_shards of every job,
+        all in one serve session; returns (Tuning, best proxy ms)."""
+        arr = (Job * len(jobs))(*jobs)
+        best = Tuning()
+        ms = ctypes.c_double()
+        r = lib().e13_autotune_jobs(self.h, arr, len(jobs), proxy_shards, ctypes.byref(start) if start else None,
+                                    ctypes.byref(best), ctypes.byref(ms))
+        if r:
+            raise E13Error(r, "e13_autotune_jobs")
         return best, ms.value
 
     def stats(self) -> Stats:

@@ -89,7 +89,8 @@ enum {
 typedef struct e13_tuning {
   int32_t kernel;            /* E13_KERNEL_* */
   int32_t block;             /* lanes (threads) per CTA: 64..768, multiple of 32 */
-  int32_t slice;             /* steps per round between warp-level refills */
+  int32_t slice;             /* iterations per round between warp-level refills; each iteration takes up
+                                to two actions (a step, a run skip, a stage test or a first read) per lane */
   int32_t warp_stack;        /* nodes in each warp's private DFS stack (persistent) */
   int32_t step_cap;          /* plain kernel: steps per work item before it is requeued */
   int32_t batch;             /* nodes taken from the frontier per launch / epoch (0 = auto: the whole
@@ -193,7 +194,9 @@ int e13_search(e13_ctx *ctx, const e13_job *job, const e13_tuning *tuning, e13_c
    nshards) searches nodes s, s + nshards, ...  The leaves, steps and survivors
    that the expansion itself finishes count in shard 0 only.  So the counts
    of all shards add up to e13_search's, and their survivors together are its
-   survivors.  Every shard must be given the same job and tuning.  nshards = 1
+   survivors.  Every shard must be given the same job; which nodes a shard
+   holds does not depend on the tuning (the expansion uses fixed settings), so
+   shards may run with different tunings.  nshards = 1
    is e13_search.  Returns as e13_search; E13_ERR_ARG for a shard out of
    range. */
 int e13_search_shard(e13_ctx *ctx, const e13_job *job, const e13_tuning *tuning, int shard, int nshards,
@@ -336,16 +339,20 @@ int e13_serve_preempt(e13_serve *s, int64_t id);
 /* Autotuner (no counterpart in the reference, which has one fixed GPU
    launch shape, src/e13gpu.py:342-346, and a fixed serial split depth,
    E13_SPLIT, src/e13search.c:47-49): coordinate descent over block size
-   (lanes per CTA, one CTA per SM), slice (actions between a warp's refill
+   (lanes per CTA, one CTA per SM), slice (iterations between a warp's refill
    rounds), warp_stack (the subtree depth a warp keeps to itself before it
-   spills to the frontier or donates) and pool_low_pct (the donation
-   threshold at which warps with deep stacks fork work off to idle warps),
-   timing the persistent kernel with CUDA events.  The proxy is shard 0 of
-   proxy_shards of the job itself (e13_search_shard; 0 or 1 = the whole job), so
-   a candidate costs about 1/proxy_shards of the job.  Each axis keeps a value
-   only if it is at least 2 % faster.  Every candidate must reproduce the same
-   counts, else E13_ERR_CUDA.  start may be NULL (defaults); *best_ms (may be
-   NULL) is the best proxy time. */
+   spills to the frontier or donates) and pool_low_pct (the donation threshold
+   at which warps with deep stacks fork work off to idle warps), timing the
+   persistent kernel with CUDA events.  The proxy is the workload itself at a
+   fraction of its cost: shard 0 of proxy_shards of each of the n jobs
+   (e13_serve_submit_shard; 0 or 1 = the whole jobs), all run together in one
+   serve session, as a workload of several jobs runs.  Each axis keeps a value
+   only if it is at least 3 % faster.  Every candidate must reproduce every
+   job's counts, else E13_ERR_CUDA.  start may be NULL (defaults); *best_ms
+   (may be NULL) is the best proxy time (epochs only). */
+int e13_autotune_jobs(e13_ctx *ctx, const e13_job *jobs, int n, int32_t proxy_shards, const e13_tuning *start,
+                      e13_tuning *best, double *best_ms);
+/* e13_autotune_jobs for one job. */
 int e13_autotune(e13_ctx *ctx, const e13_job *job, int32_t proxy_shards, const e13_tuning *start, e13_tuning *best,
                  double *best_ms);
 

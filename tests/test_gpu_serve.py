@@ -103,34 +103,35 @@ def test_preempted_jobs_resume_exactly(searches):
             for r in srv.step():
                 got[r.id] = (r, srv.survivors(r.id))
             steps += 1
-            if steps % 3 == 0:  # preempt the lowest-numbered unfinished job (a no-op while it is queued)
-                k = min(i for i in range(len(jobs)) if i not in got)
-                srv.preempt(k)
+            left = [i for i in range(len(jobs)) if i not in got]
+            if steps % 3 == 0 and left:  # preempt the lowest-numbered unfinished job (a no-op while it is queued)
+                srv.preempt(left[0])
         swaps = srv.swapped_out()
     assert swaps > 0
     _check_mix(searches, mix, jobs, got)
 
 
 def test_swap_out_when_the_frontier_runs_out_of_room(searches):
-    """A frontier capacity between one job's largest frontier and the jobs'
-    largest frontier together: after an epoch the jobs with the most live
-    nodes are swapped out by the session itself and resumed later; results
-    still equal the reference's."""
-    mix = _swap_mix(searches)
+    """A frontier with room for one epoch's outputs and 20,000 nodes more: the
+    14 FMAX = 2 jobs fit in it (a frontier node leads to at least one leaf of
+    its own, and none of them has 20,000 leaves), the FMAX = 3 job X = 11
+    (1.4e7 leaves, over 10^5 machines live at once on a full GPU) does not.  After an epoch the session swaps out the job with the most live
+    nodes, so the large job goes to host memory while the small ones finish
+    (each equal to the reference's log); alone, it still does not fit and ends
+    with E13_ERR_OVERFLOW, the session going on."""
+    mix = [(searches["local_edits_f2"], X) for X in range(14)] + [(searches["local_edits_f3"], 11)]
     jobs = [make_job(e, X) for e, X in mix]
-    block, ws = 256, 16
-    out_nodes = 2 * (148 * block // 32) * (32 + ws) + 65536  # one epoch's output room at this launch shape
-    tune = E.tuning(block=block, warp_stack=ws, epoch_us=2000)
-    with E.Server(ctx(), tune, reserve_nodes=64) as srv:  # small reservations: every job is admitted at once
-        srv.run_all(jobs)
-        peak, peak_job = srv.peaks()
-    assert peak > peak_job
-    tune.stack_nodes = out_nodes + (peak + 2 * peak_job) // 3
+    out_nodes = 2 * (148 * 768 // 32) * (32 + 256) + 65536  # one epoch's output room at the default shape
+    tune = E.tuning(epoch_us=2000, stack_nodes=out_nodes + 20000)
     with E.Server(ctx(), tune, reserve_nodes=64) as srv:
         got = srv.run_all(jobs)
         swaps = srv.swapped_out()
-    assert swaps > 0, (peak, peak_job)
-    _check_mix(searches, mix, jobs, got)
+    assert swaps > 0
+    for i, (e, X) in enumerate(mix[:-1]):
+        res, surv = got[i]
+        assert res.status == 0, (X, res.status)
+        check_entry(dict(e, expect=[_expect(e, X)]), [res.counts.as_dict()])
+    assert got[len(mix) - 1][0].status == -6  # E13_ERR_OVERFLOW
 
 
 def test_admission_reserves_by_estimate(searches):
