@@ -84,6 +84,7 @@ struct Ctl {
   int dump;                      // persistent: end the epoch now
   int busy;                      // persistent: warps holding work or claiming it
   int idle;                      // persistent: warps waiting for work (starved)
+  int deep;                      // persistent: warps holding 2 or more stack nodes (work a dump would spread)
   int error;                     // kErr* bits
   int launches;
   // utilisation counters: warp rounds, running lanes summed over rounds,

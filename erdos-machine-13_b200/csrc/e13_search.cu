@@ -209,6 +209,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   bool busy = false;           // persistent: counted in ctl->busy
   bool top_dirty = false;      // persistent: the stack top lives only in the shared copy (its HBM slot is stale)
   bool counted_idle = false;   // persistent, lane 0: this warp is counted in ctl->idle
+  bool counted_deep = false;   // persistent, lane 0: this warp is counted in ctl->deep
   const int nwarps_all = (int)(((long long)gridDim.x * stride) >> 5);
   int rounds = 0;              // slices run: a warp dumps only after one (progress every epoch)
   unsigned backoff = 256;
@@ -438,6 +439,10 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
         if (lane == 0) atomicSub(&ctl->busy, 1);
         busy = false;
       }
+      if (lane == 0 && (sp >= 2) != counted_deep) {  // (a donation below is seen next round)
+        atomicAdd(&ctl->deep, counted_deep ? -1 : 1);
+        counted_deep = !counted_deep;
+      }
       int d = 0;
       if (!has_work || (rounds & 7) == 0) {  // the control words are in L2: read them every 8th round
         if (lane == 0) {
@@ -463,15 +468,17 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
         // starving.  Work spreads inside an epoch only through donated nodes,
         // which a few deep warps hand out one at a time: a job whose subtrees
         // are shallow would run on a few warps for a long time.  When more
-        // than half of the warps wait for work, end the epoch (after a
-        // shortest length): the dump puts every warp's stack on the frontier
-        // and the next epoch deals it out over all warps.
+        // than half of the warps wait for work and some warp holds a stack
+        // of 2 or more nodes, end the epoch (after a shortest length): the
+        // dump puts every warp's stack on the frontier and the next epoch
+        // deals it out over all warps.  (With no deep stack left, the work
+        // is a few long-running machines that a dump would not spread.)
         if (lane == 0) {
           if (!counted_idle) {
             atomicAdd(&ctl->idle, 1);
             counted_idle = true;
           } else if (backoff >= 1024 && globaltimer() - t_begin > (unsigned long long)P.min_epoch_ns &&
-                     2 * *((volatile int *)&ctl->idle) > nwarps_all) {
+                     2 * *((volatile int *)&ctl->idle) > nwarps_all && *((volatile int *)&ctl->deep) > 0) {
             *((volatile int *)&ctl->dump) = 1;
           }
         }
@@ -724,6 +731,7 @@ __global__ void finish_launch(Ctl *ctl, long long cap, long long batch_max, long
   ctl->dump = 0;
   ctl->busy = 0;
   ctl->idle = 0;
+  ctl->deep = 0;
   ctl->pool_head = 0;
   ctl->pool_tail = 0;
   ctl->launches += 1;
