@@ -72,6 +72,10 @@ CPU_SAMPLE = "local_edits_f3"
 OPS_PER_STEP = 16  # integer lane-ops per simulated step (hash test 2, deadline 1, address 1, load+extract 2,
 #                    index 1, table 2, fork test 1, halt test 1, write test 1, head 2, bounds 2)
 NODE_BYTES = 320   # one frontier node (e13dev::Node)
+# DRAM bytes (read + write) of one 200 ms epoch launch of the persistent search
+# kernel on the FMAX = 4 workload, from an ncu --set full capture of this build
+# (dram__bytes_read.sum + dram__bytes_write.sum); the path is not DRAM-bound
+EPOCH_TRAFFIC = {"local_edits_f4": 986.6e6}
 
 
 def golden(name):
@@ -526,9 +530,10 @@ def main():
     value = tot["steps"] / dev_s
     sm_mhz = clocks["sm_mhz"] or 1965.0
     rl = roofline(tot["steps"], dev_s, sm_mhz, nsm)
-    rl.update({"traffic": None, "note": f"{OPS_PER_STEP} integer lane-ops per step; peak = {nsm} SMs x 128 lanes x "
-                                        f"{sm_mhz:.0f} MHz (median SM clock sampled during the timed region); "
-                                        "DRAM traffic is not the bound (see the profile summary)"})
+    rl.update({"traffic": EPOCH_TRAFFIC.get(args.workload),
+               "note": f"{OPS_PER_STEP} integer lane-ops per step; peak = {nsm} SMs x 128 lanes x {sm_mhz:.0f} MHz "
+                       "(median SM clock sampled during the timed region); traffic = DRAM bytes of one 200 ms "
+                       "epoch launch (ncu), about 5 GB/s: not the bound"})
     line = {"metric": "TM steps/s", "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot["dev_ms"] / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "int32+u64", "data": "synthetic (reference searches)",
