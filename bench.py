@@ -329,6 +329,7 @@ def serve_tuning(E, tuned, stack_nodes=0):
     t = E.tuning(epoch_us=200000, stack_nodes=stack_nodes)
     if tuned is not None:
         t.block, t.slice, t.warp_stack, t.pool_low_pct = tuned.block, tuned.slice, tuned.warp_stack, tuned.pool_low_pct
+        t.run_skip = tuned.run_skip
     return t
 
 
@@ -356,6 +357,8 @@ def run_sequential(E, ctx, jobs, kernel, tuned=None):
     t = E.tuning(kernel=kernel)
     if tuned is not None:
         t.block, t.slice, t.warp_stack, t.pool_low_pct = tuned.block, tuned.slice, tuned.warp_stack, tuned.pool_low_pct
+        if kernel == E.KERNEL_PERSISTENT:
+            t.run_skip = tuned.run_skip  # tuned on the persistent kernel; the plain one keeps the library default
     for X, job in jobs:
         c, surv = ctx.search(job, t)
         st = ctx.stats()
@@ -489,7 +492,8 @@ def main():
         tuning_cfg = {"autotuned": True, "proxy": f"shard 0 of 4 of each of the {len(jobs)} jobs, in one serve session",
                       "proxy_ms": pms,
                       "autotune_wall_s": time.perf_counter() - t0, "block": tuned.block, "slice": tuned.slice,
-                      "warp_stack": tuned.warp_stack, "pool_low_pct": tuned.pool_low_pct}
+                      "warp_stack": tuned.warp_stack, "pool_low_pct": tuned.pool_low_pct,
+                      "run_skip": tuned.run_skip}
     tune = serve_tuning(E, tuned, args.stack_nodes)
 
     for _ in range(args.warmup):

@@ -41,7 +41,7 @@ constexpr int kFlagAbs = 1, kFlagRel = 2, kFlagCs0 = 4, kFlagKeep = 32;
 // or between slices (pend = -1, one child: go on).  Children still to run: the
 // keep child (kFlagKeep) and the alternatives in vmask (bit v = move v).
 struct __align__(16) Node {
-  u64 hb;             // hash of the ones at cells >= -2
+  u64 hb;             // low 32 bits of the hash of the ones at cells >= -2 (Lane::hb)
   u64 ch[3];          // counter hash at the first stage start with c = 0, 1, 2
   u64 vmask;
   int p, st, t, deadline;  // p = head + 64
@@ -103,6 +103,37 @@ __constant__ u64 c_tgt[kStages + 2];
 __constant__ int c_deadline[kStages + 2];  // 4 * erdos_14 stage step + 64 (src/e13search.c:159)
 __constant__ int c_exc[kStages + 1];       // exceptions by stage (src/e13search.c:71)
 
+// Shared-memory key tables of the filter, in one block of kKeySmemBytes:
+// the full keys of cells < -2 (the counter hash, rebuilt from the tape at a
+// stage test), then the low and the high halves of the keys of cells >= -2
+// (zero below -2).  The step loop keeps only the low half of hb and reads
+// only `lo`; the high half is rebuilt from the tape with `hi` where a stage
+// start would be accepted (stage_check).
+struct KeyTabs {
+  u64 *c;
+  u32 *lo, *hi;
+};
+constexpr int kKeySmemBytes = 64 * 8 + kTapeCells * 8;
+
+__device__ __forceinline__ KeyTabs key_tables(unsigned char *smem) {
+  KeyTabs k;
+  k.c = reinterpret_cast<u64 *>(smem);
+  k.lo = reinterpret_cast<u32 *>(k.c + 64);
+  k.hi = k.lo + kTapeCells;
+  return k;
+}
+
+// Fills the key tables (every thread of the block takes part; the caller
+// synchronises before the first use).
+__device__ __forceinline__ void fill_key_tables(const KeyTabs &k) {
+  for (int i = threadIdx.x; i < kTapeCells; i += blockDim.x) {
+    const u64 v = (i >= kCounterCells) ? c_key[i] : 0ull;
+    k.lo[i] = (u32)v;
+    k.hi[i] = (u32)(v >> 32);
+  }
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) k.c[i] = (i < kCounterCells) ? c_key[i] : 0ull;
+}
+
 // Shared-memory copies of the stage tables: lanes of a warp index them by
 // their own stage, which constant memory would serialise.  Every kernel that
 // runs the filter fills them with load_stage_tables() before its first step.
@@ -120,10 +151,12 @@ __device__ __forceinline__ void load_stage_tables() {
 
 enum { kEvRun = 0, kEvDead = 1, kEvSurv = 2, kEvStage = 3, kEvCell = 4 };
 
-// Registers of one lane's machine.
+// Registers of one lane's machine.  hb and tgt are the low 32 bits of the
+// reference's 64-bit hb and TGT[nt]: the step loop compares those, and a
+// match goes on to the full 64-bit comparison in stage_check.
 struct Lane {
   int p, st, t, deadline, tseg, job;
-  u64 hb, tgt;
+  u32 hb, tgt;
   int nt, stage, st0, p0, flags;
   u64 ch0, ch1, ch2;
   int nintro, budget;
@@ -179,9 +212,9 @@ __device__ __forceinline__ int run_length(const u32 *__restrict__ tcol, int stri
 // also have passed the deadline test (t + i <= deadline) and the window test
 // (the head stays in 1..1362); the step that fails either test is then taken by
 // the normal loop.  Steps counted and the death point equal single-stepping.
-__device__ __forceinline__ int step_slice(int &p, int &st, int &t, const int deadline, u64 &hb, const u64 tgt,
+__device__ __forceinline__ int step_slice(int &p, int &st, int &t, const int deadline, u32 &hb, const u32 tgt,
                                           u32 *__restrict__ tcol, const u32 *__restrict__ rcol,
-                                          const u64 *__restrict__ keyb, const int stride, int &n, int &cell) {
+                                          const u32 *__restrict__ keyb, const int stride, int &n, int &cell) {
   while (n > 0) {
     if (t > deadline) return kEvDead;
     const int widx = (p >> 5) * stride;
@@ -213,7 +246,7 @@ __device__ __forceinline__ int step_slice(int &p, int &st, int &t, const int dea
     }
     if ((e ^ sym) & 1u) {
       tcol[widx] = word ^ (1u << (p & 31));
-      hb ^= keyb[p];  // zero for cells < -2: those go to the counter hash
+      hb ^= keyb[p];  // low key halves; zero for cells < -2: those go to the counter hash
     }
     p += (int)(e & 2u) - 1;
     if ((unsigned)(p - 1) >= (unsigned)(kTapeCells - 2)) return kEvDead;  // head <= -64 or >= 1299
@@ -226,23 +259,27 @@ __device__ __forceinline__ int step_slice(int &p, int &st, int &t, const int dea
 }
 
 // One action of a running lane, the unit of the warp's lock-step loop: one
-// step, one run skip, one stage test or one first-read event.  Every running
+// step, one run skip (SKIP only), one stage test or one first-read event.  Every running
 // lane of a warp takes exactly one action per iteration, so the warp stays
 // converged except inside the rare branches, which rejoin at the end of the
 // iteration.  Returns 0 (go on), kEvDead, kEvSurv or kEvCell (a cell whose
 // entry has kEntSpecial; *cell and *ecell say which).  Same semantics as
 // step_slice(): each step follows src/e13search.c:134-177 in order.
-__device__ __forceinline__ int stage_check(struct Lane &L, const u32 *tcol, const u64 *keyc, int stride);
+__device__ __forceinline__ int stage_check(struct Lane &L, const u32 *tcol, const KeyTabs &K, int stride);
 
+//
+// SKIP = false takes one step per action and leaves out the run-skip
+// arithmetic, which costs more than it saves while a warp's machines are
+// young: their runs of a self-loop are short.
+template <bool SKIP>
 __device__ __forceinline__ int lane_act(Lane &L, u32 *__restrict__ tcol, const u32 *__restrict__ rcol,
-                                        const u64 *__restrict__ keyb, const u64 *__restrict__ keyc, const int stride,
-                                        int &cell, u32 &ecell) {
+                                        const KeyTabs &K, const int stride, int &cell, u32 &ecell) {
   if (L.t > L.deadline) return kEvDead;
   const int p = L.p;
   const int widx = (p >> 5) * stride;
   const u32 word = tcol[widx];
   const u32 row = rcol[L.st * stride];
-  const u64 kk = keyb[p];  // loaded with the word and the row, used only on a flip
+  const u32 kk = K.lo[p];  // loaded with the word and the row, used only on a flip
   const u32 sym = (word >> (p & 31)) & 1u;
   const u32 e = (row >> (sym << 4)) & 0x1FFu;
   if (e & kEntSpecial) {
@@ -255,27 +292,30 @@ __device__ __forceinline__ int lane_act(Lane &L, u32 *__restrict__ tcol, const u
   // the window.  Computed without branches so the warp does not split.
   const bool right = (e & 2u) != 0;
   const int b = p & 31;
-  const u32 x = word ^ (0u - sym);             // cells holding sym are 0 bits
-  const u32 xr = right ? x : __brev(x);        // look upwards in both directions
-  const int bb = right ? b : 31 - b;
-  const u32 up = xr >> bb;
-  int k = up ? __ffs(up) - 1 : 32 - bb;
-  const int lim_t = L.deadline - L.t + 1;
-  const int room = right ? (kTapeCells - 2) - p : p - 1;
-  k = k < lim_t ? k : lim_t;
-  k = k < room ? k : room;
-  k = ((e & kEntSelf) && L.hb != L.tgt && k > 1) ? k : 1;
+  int k = 1;
+  if (SKIP) {
+    const u32 x = word ^ (0u - sym);             // cells holding sym are 0 bits
+    const u32 xr = right ? x : __brev(x);        // look upwards in both directions
+    const int bb = right ? b : 31 - b;
+    const u32 up = xr >> bb;
+    k = up ? __ffs(up) - 1 : 32 - bb;
+    const int lim_t = L.deadline - L.t + 1;
+    const int room = right ? (kTapeCells - 2) - p : p - 1;
+    k = k < lim_t ? k : lim_t;
+    k = k < room ? k : room;
+    k = ((e & kEntSelf) && L.hb != L.tgt && k > 1) ? k : 1;
+  }
   {  // the write, without a branch (a self-loop cell never flips)
     const u32 flip = (e ^ sym) & 1u;
     tcol[widx] = word ^ (flip << b);
-    L.hb ^= kk & (0ull - (u64)flip);  // keyb is zero for cells < -2: those go to the counter hash
+    L.hb ^= kk & (0u - flip);  // the key is zero for cells < -2: those go to the counter hash
   }
   const int np = p + (right ? k : -k);
   if ((unsigned)(np - 1) >= (unsigned)(kTapeCells - 2)) return kEvDead;  // head <= -64 or >= 1299
   L.p = np;
   L.st = (int)((e >> 2) & 15u);
   L.t += k;
-  if (L.hb == L.tgt) return stage_check(L, tcol, keyc, stride);
+  if (L.hb == L.tgt) return stage_check(L, tcol, K, stride);
   return 0;
 }
 
@@ -295,9 +335,29 @@ __device__ __forceinline__ u64 counter_hash(const u32 *tcol, const u64 *keyc, in
   return hc;
 }
 
-// The stage-start test of src/e13search.c:136-161 once hb matches TGT[nt].
-// Returns 0 (go on), kEvDead or kEvSurv.
-__device__ __forceinline__ int stage_check(Lane &L, const u32 *tcol, const u64 *keyc, int stride) {
+// High 32 bits of the reference's hb: the XOR of the high key halves of the
+// ones at cells >= -2, from the tape words a machine of t steps can have
+// written (cells < -2 have zero keys in `hi`).
+__device__ __forceinline__ u32 hash_hi(const u32 *tcol, const u32 *hi_keys, int stride, int t) {
+  int lo, hi;
+  tape_extent(t, lo, hi);
+  u32 h = 0;
+  for (int w = lo < 1 ? 1 : lo; w <= hi; ++w) {
+    u32 x = tcol[w * stride];
+    while (x) {
+      h ^= hi_keys[32 * w + __ffs(x) - 1];
+      x &= x - 1;
+    }
+  }
+  return h;
+}
+
+// The stage-start test of src/e13search.c:136-161 once the low 32 bits of hb
+// match TGT[nt].  The reference enters it on the full 64-bit match: the state
+// and head rules come first (they need no hash), then the high halves are
+// compared, and only then does the test act.  Returns 0 (go on), kEvDead or
+// kEvSurv.
+__device__ __forceinline__ int stage_check(Lane &L, const u32 *tcol, const KeyTabs &K, int stride) {
   const int nt = L.nt;
   if (nt > 1 && L.st != L.st0) return 0;  // the common rejection, before any load
   const int c = s_exc[nt];
@@ -307,7 +367,8 @@ __device__ __forceinline__ int stage_check(Lane &L, const u32 *tcol, const u64 *
     if (L.p - (1 << nt) != L.p0 - 2) r = 0;
     if (!a && !r) return 0;
   }
-  const u64 hc = counter_hash(tcol, keyc, stride);
+  if (hash_hi(tcol, K.hi, stride, L.t) != (u32)(s_tgt[nt] >> 32)) return 0;  // no 64-bit match: no test
+  const u64 hc = counter_hash(tcol, K.c, stride);
   const u64 chc = c == 0 ? L.ch0 : (c == 1 ? L.ch1 : L.ch2);
   if (((L.flags >> (2 + c)) & 1) && chc != hc) return kEvDead;
   if (c != 0 && (L.flags & 4) && L.ch0 == hc) return kEvDead;
@@ -326,7 +387,7 @@ __device__ __forceinline__ int stage_check(Lane &L, const u32 *tcol, const u64 *
   if (nt == kStages) return kEvSurv;
   L.nt = nt + 1;
   L.deadline = s_deadline[nt + 1];
-  L.tgt = s_tgt[nt + 1];
+  L.tgt = (u32)s_tgt[nt + 1];
   return 0;
 }
 

@@ -34,7 +34,6 @@ namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kEstBlock = 256;
-constexpr int kEstKeyBytes = (kTapeCells + 64) * 8;
 
 enum { kPrIdle = 0, kPrRun = 1, kPrFork = 2, kPrDead = 3, kPrSurv = 4 };
 
@@ -51,12 +50,12 @@ __device__ __forceinline__ u64 mix_next(u64 &s) {
 // per-step semantics as the search (lane_act, src/e13search.c:134-177); here
 // every first read is a fork, as in run() with fixed[i] == 0.
 __device__ __forceinline__ void run_to_event(Lane &L, int &status, int &fork_cell, u32 &fork_e, u32 *tcol,
-                                             const u32 *rcol, const u64 *keyb, const u64 *keyc, int stride) {
+                                             const u32 *rcol, const KeyTabs &K, int stride) {
   while (__any_sync(kFull, status == kPrRun)) {
     if (status == kPrRun) {
       int cell = 0;
       u32 e = 0;
-      const int ev = lane_act(L, tcol, rcol, keyb, keyc, stride, cell, e);
+      const int ev = lane_act<true>(L, tcol, rcol, K, stride, cell, e);
       if (ev == kEvCell) {
         if (e == kEntHalt) {
           status = kPrDead;  // a fixed halt cell
@@ -79,14 +78,12 @@ __global__ void __launch_bounds__(kEstBlock) estimate_kernel(const Node *root, i
                                                              long long nprobes, u64 seed, double *out,
                                                              unsigned long long *next_probe) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  u64 *keyb = reinterpret_cast<u64 *>(smem_raw);  // keys of cells >= -2 (0 below)
-  u64 *keyc = keyb + kTapeCells;                  // keys of cells < -2
-  u32 *tape = reinterpret_cast<u32 *>(keyc + 64);
+  const KeyTabs K = key_tables(smem_raw);
+  u32 *tape = reinterpret_cast<u32 *>(smem_raw + kKeySmemBytes);
   const int stride = blockDim.x;
   u32 *rows = tape + kTapeWords * stride;
   Node *node = reinterpret_cast<Node *>(rows + 16 * stride) + (threadIdx.x >> 5);  // this warp's path node
-  for (int i = threadIdx.x; i < kTapeCells; i += stride) keyb[i] = (i >= kCounterCells) ? c_key[i] : 0ull;
-  for (int i = threadIdx.x; i < 64; i += stride) keyc[i] = (i < kCounterCells) ? c_key[i] : 0ull;
+  fill_key_tables(K);
   load_stage_tables();
   u32 *tcol = tape + threadIdx.x;
   u32 *rcol = rows + threadIdx.x;
@@ -117,7 +114,7 @@ __global__ void __launch_bounds__(kEstBlock) estimate_kernel(const Node *root, i
       lane_load(L, root, tcol, rcol, stride, 0);
       status = kPrRun;
     }
-    run_to_event(L, status, fork_cell, fork_e, tcol, rcol, keyb, keyc, stride);
+    run_to_event(L, status, fork_cell, fork_e, tcol, rcol, K, stride);
     if (lane == 0) {
       o_nodes += 1.0;
       o_steps += (double)L.t;
@@ -152,7 +149,7 @@ __global__ void __launch_bounds__(kEstBlock) estimate_kernel(const Node *root, i
           t0 = L.t;
           status = kPrRun;
         }
-        run_to_event(L, status, fork_cell, fork_e, tcol, rcol, keyb, keyc, stride);
+        run_to_event(L, status, fork_cell, fork_e, tcol, rcol, K, stride);
         // weighted counts, added in child order as the reference does
         const int nb = min(32, k - 32 * b);
         for (int j = 0; j < nb; ++j) {
@@ -194,7 +191,7 @@ __global__ void __launch_bounds__(kEstBlock) estimate_kernel(const Node *root, i
           apply_child(L, node, ch, rcol, stride, sym_lo, sym_hi, true);
           status = kPrRun;
         }
-        run_to_event(L, status, fork_cell, fork_e, tcol, rcol, keyb, keyc, stride);
+        run_to_event(L, status, fork_cell, fork_e, tcol, rcol, K, stride);
       }
       __syncwarp();  // every lane is done reading the old path node
       if (lane == holder) {
@@ -237,7 +234,7 @@ extern "C" int e13_estimate(e13_ctx *ctx, const e13_job *job, int64_t probes, ui
   if (upload_filter_tables() != cudaSuccess) return E13_ERR_CUDA;
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e13_ctx_device(ctx));
-  const size_t smem = kEstKeyBytes + (size_t)(kTapeWords + 16) * kEstBlock * 4 + (size_t)(kEstBlock / 32) * sizeof(Node);
+  const size_t smem = kKeySmemBytes + (size_t)(kTapeWords + 16) * kEstBlock * 4 + (size_t)(kEstBlock / 32) * sizeof(Node);
   if (cudaFuncSetAttribute(estimate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return E13_ERR_CUDA;
 

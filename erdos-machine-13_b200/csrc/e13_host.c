@@ -174,7 +174,7 @@ void e13_default_tuning(e13_tuning *t) {
   t->epoch_us = 200000;
   t->epochs_per_graph = 4;
   t->pool_low_pct = 5;
-  t->run_skip = 1;
+  t->run_skip = 8192;
   t->stack_nodes = 0;
 }
 
@@ -185,7 +185,7 @@ int e13_resolve_tuning(const e13_tuning *in, int serve, e13_tuning *out) {
   if (serve) t.epoch_us = 10000; /* short epochs: jobs join and leave at every epoch boundary */
   if (in) {
     if (in->kernel != E13_KERNEL_PLAIN && in->kernel != E13_KERNEL_PERSISTENT) return E13_ERR_ARG;
-    if (in->run_skip != 0 && in->run_skip != 1) return E13_ERR_ARG;
+    if (in->run_skip < 0) return E13_ERR_ARG;
     if (in->block < 0 || in->slice < 0 || in->warp_stack < 0 || in->step_cap < 0 || in->batch < 0 ||
         in->epoch_us < 0 || in->epochs_per_graph < 0 || in->pool_low_pct < 0 || in->stack_nodes < 0)
       return E13_ERR_ARG;

@@ -19,7 +19,7 @@ __device__ __forceinline__ void lane_load(Lane &L, const Node *N, u32 *tcol, u32
   L.st = N->st;
   L.t = N->t;
   L.deadline = N->deadline;
-  L.hb = N->hb;
+  L.hb = (u32)N->hb;
   L.nt = N->nt;
   L.stage = N->stage;
   L.st0 = N->st0;
@@ -31,7 +31,7 @@ __device__ __forceinline__ void lane_load(Lane &L, const Node *N, u32 *tcol, u32
   L.nintro = N->nintro;
   L.budget = N->budget;
   L.job = N->job;
-  L.tgt = s_tgt[L.nt];
+  L.tgt = (u32)s_tgt[L.nt];
   L.tseg = L.t;
   const uint4 *rv = reinterpret_cast<const uint4 *>(N->cellv);
   for (int k = 0; k < 4; ++k) {  // all 16 rows: states >= nq hold halts

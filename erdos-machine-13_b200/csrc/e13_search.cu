@@ -46,7 +46,6 @@ using namespace e13dev;
 namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
-constexpr int kKeySmemBytes = (kTapeCells + 64) * 8;
 constexpr long long kPoolNodes = 1LL << 18;  // donation pool: 256 Ki nodes (80 MiB)
 constexpr long long kWholeFrontier = 1LL << 62;  // persistent batch when e13_tuning::batch is 0
 constexpr long long kPoolWaitNs = 200000000;     // 200 ms: a donor publishes a claimed slot within microseconds
@@ -59,6 +58,7 @@ struct Params {
   unsigned long long *jobcnt;  // kMaxJobs x kJobCounters totals
   int nq;
   int slice, step_cap, wdepth, pool_low, run_skip;
+  int skip_after;            // run skip only in slices of warps with a machine of at least this many steps
   long long out_cap, out_soft, surv_cap, pool_cap;
   long long epoch_ns;
   long long wait_ns;         // persistent: limit of the wait for a claimed pool slot's data
@@ -140,9 +140,8 @@ __device__ __forceinline__ int wrap(int s, int d) { return s >= d ? s - d : s; }
 template <bool PERSIST>
 __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  u64 *keyb = reinterpret_cast<u64 *>(smem_raw);  // keys of cells >= -2 (0 below)
-  u64 *keyc = keyb + kTapeCells;                  // keys of cells < -2
-  u32 *tape = reinterpret_cast<u32 *>(keyc + 64);
+  const KeyTabs K = key_tables(smem_raw);
+  u32 *tape = reinterpret_cast<u32 *>(smem_raw + kKeySmemBytes);
   const int stride = blockDim.x;
   u32 *rows = tape + kTapeWords * stride;
   // persistent: a shared-memory copy of each warp's current stack-top node, so
@@ -151,8 +150,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
   __shared__ int4 s_jp[kMaxJobs];                              // per-job moves and symmetry range
   __shared__ unsigned long long s_jc[kMaxJobs][kJobCounters];  // per-job leaves, steps, deaths by stage
 
-  for (int i = threadIdx.x; i < kTapeCells; i += stride) keyb[i] = (i >= kCounterCells) ? c_key[i] : 0ull;
-  for (int i = threadIdx.x; i < 64; i += stride) keyc[i] = (i < kCounterCells) ? c_key[i] : 0ull;
+  fill_key_tables(K);
   if (threadIdx.x < kMaxJobs) {
     const JobParam jp = P.jobs[threadIdx.x];
     s_jp[threadIdx.x] = make_int4(jp.nv, jp.sym_lo, jp.sym_hi, 0);
@@ -544,6 +542,10 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
     ++rounds;
     {
       const unsigned rm = __ballot_sync(kFull, status == kStRun);
+      // word-at-a-time run skips pay off only for machines that have built
+      // long runs: the warp uses them in this slice when one of its machines
+      // has run skip_after steps (a warp-uniform choice: no divergence)
+      const bool skip_w = P.run_skip && __any_sync(kFull, status == kStRun && L.t >= P.skip_after);
       st_lane_rounds += __popc(rm);
       if (rm) {
 #pragma unroll 1
@@ -553,8 +555,14 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
             u32 e = 0;
             // two actions per iteration: the loop control and the event
             // dispatch below are paid once for both
-            int ev = lane_act(L, tcol, rcol, keyb, keyc, stride, cell, e);
-            if (!ev) ev = lane_act(L, tcol, rcol, keyb, keyc, stride, cell, e);
+            int ev;
+            if (skip_w) {
+              ev = lane_act<true>(L, tcol, rcol, K, stride, cell, e);
+              if (!ev) ev = lane_act<true>(L, tcol, rcol, K, stride, cell, e);
+            } else {
+              ev = lane_act<false>(L, tcol, rcol, K, stride, cell, e);
+              if (!ev) ev = lane_act<false>(L, tcol, rcol, K, stride, cell, e);
+            }
             if (ev == kEvCell) {
               if (e == kEntHalt) {
                 ev = kEvDead;
@@ -740,13 +748,11 @@ __global__ void finish_launch(Ctl *ctl, long long cap, long long batch_max, long
 // Whole-table runs (src/e13search.c:428-433): one machine per thread.
 __global__ void __launch_bounds__(256) run_full_kernel(const int *tabs, int n, int nq, long long *out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  u64 *keyb = reinterpret_cast<u64 *>(smem_raw);
-  u64 *keyc = keyb + kTapeCells;
-  u32 *tape = reinterpret_cast<u32 *>(keyc + 64);
+  const KeyTabs K = key_tables(smem_raw);
+  u32 *tape = reinterpret_cast<u32 *>(smem_raw + kKeySmemBytes);
   const int stride = blockDim.x;
   u32 *rows = tape + kTapeWords * stride;
-  for (int i = threadIdx.x; i < kTapeCells; i += stride) keyb[i] = (i >= kCounterCells) ? c_key[i] : 0ull;
-  for (int i = threadIdx.x; i < 64; i += stride) keyc[i] = (i < kCounterCells) ? c_key[i] : 0ull;
+  fill_key_tables(K);
   load_stage_tables();
   __syncthreads();
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -764,14 +770,14 @@ __global__ void __launch_bounds__(256) run_full_kernel(const int *tabs, int n, i
     rcol[s * stride] = cell_slot(2 * s, e0, true) | (cell_slot(2 * s + 1, e1, true) << 16);
   }
   Lane L;
-  L.p = kLeft; L.st = 0; L.t = 0; L.deadline = s_deadline[1]; L.hb = 0; L.tgt = s_tgt[1];
+  L.p = kLeft; L.st = 0; L.t = 0; L.deadline = s_deadline[1]; L.hb = 0; L.tgt = (u32)s_tgt[1];
   L.nt = 1; L.stage = 0; L.st0 = -1; L.p0 = kLeft; L.flags = 3; L.ch0 = L.ch1 = L.ch2 = 0;  // head0 = 0 until stage 1
   int ev;
   for (;;) {
     int nn = 1 << 30, cell = 0;
-    ev = step_slice(L.p, L.st, L.t, L.deadline, L.hb, L.tgt, tcol, rcol, keyb, stride, nn, cell);
+    ev = step_slice(L.p, L.st, L.t, L.deadline, L.hb, L.tgt, tcol, rcol, K.lo, stride, nn, cell);
     if (ev == kEvStage) {
-      ev = stage_check(L, tcol, keyc, stride);
+      ev = stage_check(L, tcol, K, stride);
       if (ev == 0) continue;
     }
     if (ev == kEvCell) ev = kEvDead;  // only halts are special here
@@ -955,6 +961,9 @@ static Params make_params(const e13_ctx *c, const e13_tuning &tu, int nq, long l
   P.nq = nq;
   P.slice = tu.slice;
   P.run_skip = tu.run_skip ? 1 : 0;
+  // the plain kernel's launches wait for their slowest lane, which is the
+  // oldest machine: it skips in every slice
+  P.skip_after = (tu.run_skip >= 2 && tu.kernel == E13_KERNEL_PERSISTENT) ? tu.run_skip : 0;
   P.step_cap = tu.step_cap;
   P.wdepth = tu.warp_stack;
   P.pool_low = (int)std::max<long long>(1, nwarps * tu.pool_low_pct / 100);
@@ -989,7 +998,7 @@ static size_t search_smem(int block) {
 
 namespace {
 
-constexpr char kCkptMagic[8] = {'E', '1', '3', 'C', 'K', 'P', 'T', '1'};
+constexpr char kCkptMagic[8] = {'E', '1', '3', 'C', 'K', 'P', 'T', '2'};  // 2: Node::hb holds the low 32 bits
 constexpr long long kCkptChunk = 1LL << 16;  // nodes per host transfer (20 MiB)
 
 struct CkptHeader {
@@ -1697,8 +1706,10 @@ extern "C" int e13_autotune_jobs(e13_ctx *c, const e13_job *jobs, int n, int32_t
   // block: lanes per CTA (one CTA per SM); slice: iterations between a
   // warp's refill rounds; warp_stack: the depth of subtree a warp keeps to
   // itself before it spills or donates; pool_low_pct: the threshold below
-  // which warps with deep stacks fork work off to idle warps
+  // which warps with deep stacks fork work off to idle warps; run_skip: the
+  // machine age (steps) from which a warp takes word-at-a-time run skips
   const Axis axes[] = {
+      {&e13_tuning::run_skip, {1, 1024, 4096, 8192, 32768}, 5},
       {&e13_tuning::block, {512, 640, 768, 0, 0}, 3},
       {&e13_tuning::slice, {6, 8, 12, 16, 24}, 5},
       {&e13_tuning::warp_stack, {64, 128, 256, 512, 0}, 4},

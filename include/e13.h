@@ -98,7 +98,11 @@ typedef struct e13_tuning {
   int32_t epoch_us;          /* persistent: wall-clock bound of one epoch, microseconds */
   int32_t epochs_per_graph;  /* persistent: epochs captured in one CUDA graph */
   int32_t pool_low_pct;      /* persistent: warps donate stack nodes while the pool holds fewer than this % of warps */
-  int32_t run_skip;          /* 1: advance whole words across runs of a self-loop (exact) */
+  int32_t run_skip;          /* advance whole tape words across runs of a self-loop (exact in every form):
+                                0 never, 1 always, N >= 2 in the slices of warps where some running
+                                machine has made N steps or more (younger machines' runs are short;
+                                persistent kernel only: the plain kernel takes N >= 2 as 1, since
+                                each of its launches waits for its oldest machine) */
   int64_t stack_nodes;       /* frontier stack capacity in nodes (0 = auto) */
 } e13_tuning;
 
@@ -161,7 +165,7 @@ void e13_default_tuning(e13_tuning *t);
    the defaults, overridden by the nonzero fields of `in` (NULL: defaults; a
    serve session defaults to 10 ms epochs and always uses the persistent
    kernel).  Returns E13_ERR_ARG, and leaves *out alone, unless every field is
-   in range: kernel 0..1, run_skip 0..1, block 64..768 and a multiple of 32,
+   in range: kernel 0..1, run_skip >= 0, block 64..768 and a multiple of 32,
    slice 1..4096, warp_stack 1..4096, epoch_us 1..6e7, epochs_per_graph 1..64,
    pool_low_pct 1..100, and step_cap, batch, stack_nodes >= 0.  Every
    entry point that takes a tuning applies this check first.  No counterpart

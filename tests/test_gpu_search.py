@@ -144,14 +144,17 @@ def test_survivor_cap_reports_overflow(searches):
 
 
 @pytest.mark.parametrize("name", ["local_edits_f2", "split_test_free", "counters_f2_base_07"])
-def test_run_skip_is_exact(searches, name):
-    """Advancing whole words across a self-loop run gives the same counts,
-    steps and survivors as single steps."""
+@pytest.mark.parametrize("kernel", [E.KERNEL_PERSISTENT, E.KERNEL_PLAIN])
+def test_run_skip_is_exact(searches, name, kernel):
+    """Advancing whole words across a self-loop run (always, or only in the
+    slices of warps with an old machine) gives the same counts, steps and
+    survivors as single steps."""
     e = searches[name]
-    a = run_entry(e, E.tuning(run_skip=0))
-    b = run_entry(e, E.tuning(run_skip=1))
-    assert a == b
-    check_entry(e, b[0])
+    a = run_entry(e, E.tuning(kernel=kernel, run_skip=0))
+    for rs in (1, 100, 4096):
+        b = run_entry(e, E.tuning(kernel=kernel, run_skip=rs))
+        assert a == b, rs
+    check_entry(e, a[0])
 
 
 def test_raw_simulator_vs_oracle():

@@ -270,7 +270,7 @@ def test_tuning_ranges_are_checked():
     bad = [dict(epoch_us=-1), dict(epochs_per_graph=-1), dict(pool_low_pct=-5), dict(pool_low_pct=101),
            dict(block=48), dict(block=800), dict(block=100), dict(slice=-1), dict(slice=5000),
            dict(warp_stack=-2), dict(warp_stack=5000), dict(epochs_per_graph=65), dict(epoch_us=60_000_001),
-           dict(step_cap=-1), dict(batch=-1), dict(stack_nodes=-1), dict(kernel=2), dict(run_skip=2)]
+           dict(step_cap=-1), dict(batch=-1), dict(stack_nodes=-1), dict(kernel=2), dict(run_skip=-1)]
     for kw in bad:
         for serve in (False, True):
             r, _ = E.resolve_tuning(E.tuning(**kw), serve=serve)
