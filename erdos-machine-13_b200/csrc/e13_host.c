@@ -167,7 +167,7 @@ void e13_default_tuning(e13_tuning *t) {
   memset(t, 0, sizeof *t);
   t->kernel = E13_KERNEL_PERSISTENT;
   t->block = 768;
-  t->slice = 12;  /* iterations of two actions each */
+  t->slice = 24;  /* iterations of two actions each */
   t->warp_stack = 256;
   t->step_cap = 20000;
   t->batch = 0;

@@ -1711,7 +1711,7 @@ extern "C" int e13_autotune_jobs(e13_ctx *c, const e13_job *jobs, int n, int32_t
   const Axis axes[] = {
       {&e13_tuning::run_skip, {1, 1024, 4096, 8192, 32768}, 5},
       {&e13_tuning::block, {512, 640, 768, 0, 0}, 3},
-      {&e13_tuning::slice, {6, 8, 12, 16, 24}, 5},
+      {&e13_tuning::slice, {8, 12, 16, 24, 32}, 5},
       {&e13_tuning::warp_stack, {64, 128, 256, 512, 0}, 4},
       {&e13_tuning::pool_low_pct, {2, 5, 12, 25, 0}, 4},
   };
