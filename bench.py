@@ -75,7 +75,7 @@ NODE_BYTES = 320   # one frontier node (e13dev::Node)
 # DRAM bytes (read + write) of one 200 ms epoch launch of the persistent search
 # kernel on the FMAX = 4 workload, from an ncu --set full capture of this build
 # (dram__bytes_read.sum + dram__bytes_write.sum); the path is not DRAM-bound
-EPOCH_TRAFFIC = {"local_edits_f4": 986.6e6}
+EPOCH_TRAFFIC = {"local_edits_f4": 1807.9e6}
 
 
 def golden(name):
@@ -537,7 +537,7 @@ def main():
     rl.update({"traffic": EPOCH_TRAFFIC.get(args.workload),
                "note": f"{OPS_PER_STEP} integer lane-ops per step; peak = {nsm} SMs x 128 lanes x {sm_mhz:.0f} MHz "
                        "(median SM clock sampled during the timed region); traffic = DRAM bytes of one 200 ms "
-                       "epoch launch (ncu), about 5 GB/s: not the bound"})
+                       "epoch launch (ncu), about 9 GB/s: not the bound"})
     line = {"metric": "TM steps/s", "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot["dev_ms"] / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "int32+u64", "data": "synthetic (reference searches)",

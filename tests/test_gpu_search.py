@@ -212,8 +212,9 @@ def test_autotune_keeps_results(searches):
     e = searches["local_edits_f3"]
     job = __import__("gpu_common").make_job(e, 12)
     best, ms = ctx().autotune(job, proxy_shards=4)
-    assert ms > 0 and best.block in (512, 640, 768) and best.slice in (6, 8, 12, 16, 24)
+    assert ms > 0 and best.block in (512, 640, 768) and best.slice in (8, 12, 16, 24, 32)
     assert best.warp_stack in (64, 128, 256, 512) and best.pool_low_pct in (2, 5, 12, 25)
+    assert best.run_skip in (1, 1024, 4096, 8192, 32768)
     c, _ = ctx().search(job, best)
     exp = e["expect"][12]
     assert c.leaves == exp["leaves"] and list(c.hist) == exp["hist"] and c.steps == exp["steps"]
