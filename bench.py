@@ -24,6 +24,8 @@ with leaves/s beside it.
             one after another on both kernels (like for like)
   serving   the serving mix: a seeded Poisson stream of 40 jobs (p50/p99)
   raw_set   the raw-simulator set: 1e6 random 13-state machines, <= 2^18 steps
+  pipeline  the counter search's survivors fed into the device recheck to
+            stage 15 (enumeration feeding the deep check)
 
 Every measured search is checked against the reference's logs (leaves,
 survivors, deaths per stage, steps where logged, sorted survivor lines).
@@ -453,6 +455,30 @@ def raw_set(E, ctx):
             "note": "1e6 random 13-state tables from seed 0, <= 2^18 steps, no filter; tables drawn on the device"}
 
 
+def pipeline(E, ctx):
+    """Enumeration feeding the deep check (the division config's pipeline, on
+    the counter search: its survivors are known and the reference recheck's
+    verdicts on them are a committed fixture): the persistent search, then
+    its survivor records straight into the device recheck to stage 15."""
+    w = WORKLOADS["counter_sym"]
+    (_, job), = make_jobs(E, w)
+    t0 = time.perf_counter()
+    c, surv = ctx.search(job, E.tuning(kernel=E.KERNEL_PERSISTENT))
+    t1 = time.perf_counter()
+    pairs = sorted((E.survivor_line(job, s), s) for s in surv)
+    outs = ctx.check([E.survivor_check_in(job, s) for _, s in pairs], 15, 0)
+    t2 = time.perf_counter()
+    got = [f"{k + 1}: {E.format_recheck(o, 15)}" for k, o in enumerate(outs)]
+    with open(os.path.join(GOLD, "recheck15_counter_sym.txt")) as f:
+        ref = f.read().splitlines()
+    return {"workload": w["desc"] + ", then recheck to stage 15 of every survivor", "survivors": len(surv),
+            "search_s": t1 - t0, "check_s": t2 - t1,
+            "consistent": sum(1 for g in got if g.split(": ", 1)[1].startswith("CONSISTENT")),
+            "parity_survivor_lines": [l for l, _ in pairs] == golden_lines(golden("counter_sym")),
+            "parity_verdicts": got == ref,
+            "note": "host clock; the reference's recheck takes about 330 s on one core for these 61 machines"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -557,6 +583,7 @@ def main():
         serving_stats(E, ctx, stream)  # warm-up of the stream's job shapes
         line["serving"] = serving_stats(E, ctx, stream)
         line["raw_set"] = raw_set(E, ctx)
+        line["pipeline"] = pipeline(E, ctx)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sw = WORKLOADS[CPU_SAMPLE]

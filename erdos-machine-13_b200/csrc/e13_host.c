@@ -255,6 +255,27 @@ int e13_parse_survivor_line(const char *line, e13_check_in *in) {
   return 1;
 }
 
+int e13_survivor_check_in(const e13_job *job, const e13_survivor *s, e13_check_in *in) {
+  if (!job || !s || !in || job->nq < 1 || job->nq > E13_MAXQ) return E13_ERR_ARG;
+  memset(in, 0, sizeof *in);
+  in->nq = job->nq;
+  in->st0 = s->st0;
+  in->head0 = s->head0;
+  in->rel = !s->abs_ok && s->rel_ok;
+  for (int i = 0; i < 2 * job->nq; i++) {
+    const int c = s->tab[i];
+    if (c < 0) {  /* halt or free cell: "---", never read when '?' */
+      in->kind[i] = ((s->read_mask >> i) & 1u) ? 1 : 2;
+    } else {
+      in->kind[i] = 0;
+      in->write[i] = (int8_t)(c & 1);
+      in->move[i] = (c & 2) ? 1 : -1;
+      in->next[i] = (int8_t)(c >> 2);
+    }
+  }
+  return E13_OK;
+}
+
 /* counter set of stage n as recheck prints it: "-3,-5," ("" = none) */
 static int counter_text(const e13_check_out *o, int n, char *b, size_t len) {
   int w = 0;

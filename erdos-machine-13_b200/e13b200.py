@@ -172,6 +172,7 @@ def lib():
         L.e13_raw_run.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int64, I,
                                   ctypes.c_int64, P(ctypes.c_int64), P(ctypes.c_uint64)]
         L.e13_parse_survivor_line.argtypes = [ctypes.c_char_p, P(CheckIn)]
+        L.e13_survivor_check_in.argtypes = [P(Job), P(Survivor), P(CheckIn)]
         L.e13_format_recheck.argtypes = [P(CheckOut), I, ctypes.c_char_p, ctypes.c_size_t]
         L.e13_format_deep.argtypes = [P(CheckIn), P(CheckOut), I, ctypes.c_char_p, ctypes.c_size_t]
         _lib = L
@@ -184,7 +185,8 @@ EXPORTED = ["e13_keys", "e13_parse_cell", "e13_load_machine", "e13_parse_machine
             "e13_format_recheck", "e13_format_deep", "e13_check_crafted", "e13_raw_run", "e13_autotune", "e13_check_noalloc",
             "e13_serve_create", "e13_serve_destroy", "e13_serve_clock", "e13_serve_submit", "e13_serve_step",
             "e13_serve_pending", "e13_serve_survivors", "e13_serve_stats", "e13_resolve_tuning",
-            "e13_selftest_pool_wait", "e13_serve_submit_shard", "e13_serve_preempt", "e13_autotune_jobs"]
+            "e13_selftest_pool_wait", "e13_serve_submit_shard", "e13_serve_preempt", "e13_autotune_jobs",
+            "e13_survivor_check_in"]
 
 
 def keys():
@@ -414,6 +416,15 @@ def summary_line(job: Job, c: Counts, wall: float) -> str:
 def parse_survivor_line(line: str) -> CheckIn | None:
     ci = CheckIn()
     return ci if lib().e13_parse_survivor_line(line.encode(), ctypes.byref(ci)) else None
+
+
+def survivor_check_in(job: Job, s: Survivor) -> CheckIn:
+    """The checker input of a survivor a search returned (e13_survivor_check_in)."""
+    ci = CheckIn()
+    r = lib().e13_survivor_check_in(ctypes.byref(job), ctypes.byref(s), ctypes.byref(ci))
+    if r:
+        raise E13Error(r, "e13_survivor_check_in")
+    return ci
 
 
 def format_recheck(o: CheckOut, nmax: int) -> str:

@@ -466,6 +466,12 @@ int e13_check_noalloc(int device, const e13_check_in *in, int n, int nmax, int m
    Returns 1 on success, 0 if the line has no table. */
 int e13_parse_survivor_line(const char *line, e13_check_in *in);
 
+/* The checker input of a survivor that a search returned, without going
+   through its text: the same input e13_parse_survivor_line gives for the line
+   e13_format_survivor prints (the reference pipes e13search's SURVIVOR lines
+   into recheck / deep, src/recheck.c:28-56).  Returns E13_OK or E13_ERR_ARG. */
+int e13_survivor_check_in(const e13_job *job, const e13_survivor *s, e13_check_in *in);
+
 /* ---- check.py: stages to 11 and crafted stage starts ---- */
 
 #define E13_CRAFTED_MAX_CELLS 256  /* counter cells recorded per stage start */

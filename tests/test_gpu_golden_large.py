@@ -10,11 +10,18 @@ test run on one B200.
                    (results/5_counter_plus/extra_cell/log_cx_C1.txt, surv_cx_C1.txt)
   61 x FMAX 2 / 3  the neighbourhoods of the 61 three-state counters
                    (results/5_counter_plus/f2_f3/log_f{2,3}_all.txt)
+
+and the survivor pipeline on the device: the counter search's survivors,
+as the search returns them, go straight into the hash-free deep check to
+stage 15, whose verdicts must equal the reference recheck's
+(golden/recheck15_counter_sym.txt, made by make_pipeline_golden.py).
 """
+import os
+
 import pytest
 
 import e13b200 as E
-from gpu_common import check_entry, golden_lines, run_entry
+from gpu_common import GOLD, check_entry, ctx, golden_lines, make_job, run_entry
 
 pytestmark = pytest.mark.gpu
 
@@ -65,3 +72,22 @@ def test_counter_neighbourhoods_f3(searches):
     for n in names:
         per_x, _ = run_entry(searches[n], E.tuning(kernel=E.KERNEL_PERSISTENT))
         check_entry(searches[n], per_x)
+
+
+@pytest.mark.slow
+def test_counter_search_feeds_the_deep_check(searches):
+    """Enumeration feeding the deep check: the 61 survivors of the counter
+    search with symmetry, taken from e13_search's records with
+    e13_survivor_check_in (no text in between), are rechecked on the device
+    to stage 15; the verdicts, in sorted survivor-line order, equal the
+    reference recheck's on the reference's survivor file."""
+    e = searches["counter_sym"]
+    job = make_job(e, 13)
+    c, surv = ctx().search(job, E.tuning(kernel=E.KERNEL_PERSISTENT))
+    assert c.survivors == 61 and len(surv) == 61
+    pairs = sorted((E.survivor_line(job, s), s) for s in surv)
+    assert [l for l, _ in pairs] == golden_lines(e)
+    outs = ctx().check([E.survivor_check_in(job, s) for _, s in pairs], 15, 0)  # mode 0: recheck.c
+    got = [f"{k + 1}: {E.format_recheck(o, 15)}" for k, o in enumerate(outs)]
+    with open(os.path.join(GOLD, "recheck15_counter_sym.txt")) as f:
+        assert got == f.read().splitlines()

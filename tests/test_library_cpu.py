@@ -85,6 +85,32 @@ def test_format_survivor_matches_reference_text():
     assert E.survivor_line(job, s) == line
 
 
+def test_survivor_check_in_equals_parsed_line():
+    """e13_survivor_check_in gives the checker input that parsing the
+    survivor's printed line gives, on 300 random survivor records (moves,
+    halts, free cells, read masks, both head rules)."""
+    import random
+
+    rng = random.Random(5)
+    base = O.load_machine("erdos_14.txt")
+    _, job = E.setup(base, 9, free_cells=["F0", "F1", "G0", "G1", "H0", "H1", "I0", "I1"], lo=3, hi=9)
+    fields = ("nq", "st0", "rel", "head0")
+    for _ in range(300):
+        s = E.Survivor()
+        for i in range(2 * job.nq):
+            r = rng.random()
+            s.tab[i] = E.E13_FREE if r < 0.1 else (-1 if r < 0.2 else rng.randrange(4 * job.nq))
+        s.read_mask = rng.getrandbits(26)
+        s.st0, s.head0 = rng.randrange(job.nq), rng.randrange(-40, 3)
+        s.abs_ok, s.rel_ok = rng.randrange(2), rng.randrange(2)
+        s.steps = rng.randrange(1, 1 << 20)
+        a = E.survivor_check_in(job, s)
+        b = E.parse_survivor_line(E.survivor_line(job, s))
+        assert [getattr(a, f) for f in fields] == [getattr(b, f) for f in fields]
+        for arr in ("kind", "write", "move", "next"):
+            assert list(getattr(a, arr)) == list(getattr(b, arr)), arr
+
+
 def test_summary_format():
     base = O.load_machine("erdos_14.txt")
     _, job = E.setup(base, 9, free_cells=["F0", "F1", "G0", "G1", "H0", "H1", "I0", "I1"], lo=3, hi=9)
