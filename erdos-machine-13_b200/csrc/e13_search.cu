@@ -50,6 +50,13 @@ constexpr long long kPoolNodes = 1LL << 18;  // donation pool: 256 Ki nodes (80 
 constexpr long long kWholeFrontier = 1LL << 62;  // persistent batch when e13_tuning::batch is 0
 constexpr long long kPoolWaitNs = 200000000;     // 200 ms: a donor publishes a claimed slot within microseconds
 constexpr long long kMinEpochNs = 200000;        // 200 us: the shortest epoch a starvation dump may end
+// A warp with at most kLoneLanes running machines (the tail of a search:
+// a few long machines, the rest of the GPU idle) runs each of them in the
+// tight single-machine loop step_slice, up to kLoneSteps steps per
+// iteration: its speed is then bound by one machine's dependent chain, not
+// by issue slots, and the lock-step loop's control would only lengthen it.
+constexpr int kLoneLanes = 2;
+constexpr int kLoneSteps = 512;
 
 // steps a lane gets between warp-level refill rounds is Params::slice
 
@@ -546,6 +553,7 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
       // long runs: the warp uses them in this slice when one of its machines
       // has run skip_after steps (a warp-uniform choice: no divergence)
       const bool skip_w = P.run_skip && __any_sync(kFull, status == kStRun && L.t >= P.skip_after);
+      const bool lone_w = __popc(rm) <= kLoneLanes;
       st_lane_rounds += __popc(rm);
       if (rm) {
 #pragma unroll 1
@@ -556,7 +564,17 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
             // two actions per iteration: the loop control and the event
             // dispatch below are paid once for both
             int ev;
-            if (skip_w) {
+            if (lone_w) {
+              // the same steps and events as lane_act (step_slice follows
+              // src/e13search.c:134-177 too), the stage test between steps
+              int n = kLoneSteps;
+              ev = step_slice(L.p, L.st, L.t, L.deadline, L.hb, L.tgt, tcol, rcol, K.lo, stride, n, cell);
+              while (ev == kEvStage) {
+                ev = stage_check(L, tcol, K, stride);
+                if (ev == 0 && n > 0) ev = step_slice(L.p, L.st, L.t, L.deadline, L.hb, L.tgt, tcol, rcol, K.lo, stride, n, cell);
+              }
+              if (ev == kEvCell) e = get_entry(rcol, stride, cell);
+            } else if (skip_w) {
               ev = lane_act<true>(L, tcol, rcol, K, stride, cell, e);
               if (!ev) ev = lane_act<true>(L, tcol, rcol, K, stride, cell, e);
             } else {
