@@ -456,10 +456,11 @@ def raw_set(E, ctx):
 
 
 def pipeline(E, ctx):
-    """Enumeration feeding the deep check (the division config's pipeline, on
-    the counter search: its survivors are known and the reference recheck's
-    verdicts on them are a committed fixture): the persistent search, then
-    its survivor records straight into the device recheck to stage 15."""
+    """Enumeration feeding the deep check, the survivor pipeline of the
+    division searches, shown on the counter search (its survivors are known
+    and the reference recheck's verdicts on them are a committed fixture):
+    the persistent search, then its survivor records straight into the
+    device recheck to stage 15."""
     w = WORKLOADS["counter_sym"]
     (_, job), = make_jobs(E, w)
     t0 = time.perf_counter()
