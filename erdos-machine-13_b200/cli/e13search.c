@@ -58,8 +58,9 @@ static void maybe_autotune(e13_ctx *ctx, const e13_job *jobs, int n, e13_tuning 
     fprintf(stderr, "autotune failed (error %d): default tuning kept\n", rc);
     return;
   }
-  fprintf(stderr, "autotune jobs=%d proxy=1/%d: block=%d slice=%d warp_stack=%d pool_low_pct=%d (%.1f ms)\n", n,
-          atoi(a), best.block, best.slice, best.warp_stack, best.pool_low_pct, ms);
+  fprintf(stderr,
+          "autotune jobs=%d proxy=1/%d: block=%d slice=%d warp_stack=%d pool_low_pct=%d run_skip=%d (%.1f ms)\n", n,
+          atoi(a), best.block, best.slice, best.warp_stack, best.pool_low_pct, best.run_skip, ms);
   *tu = best;
 }
 

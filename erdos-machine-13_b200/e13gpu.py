@@ -10,7 +10,8 @@ kernel:
            "X=.. budget=0 gpu leaves=.. survivors=.. steps=.. wall=..s
            dead-at-stage(0..9): ..." and the "launches= peak stack=" line
   E13_CKPT, E13_CKPT_SEC, <E13_CKPT>.stop   checkpoints, clean stop (exit 3)
-  E13_SLICE  actions per lane between refill rounds (the kernel's slice)
+  E13_SLICE  iterations (of up to two actions per lane) between refill rounds
+             (the kernel's slice)
   E13_DEVICE the CUDA device (default 0)
 
 One difference: with X = -1 (nothing deleted) the reference driver renumbers
