@@ -202,13 +202,16 @@ __device__ __forceinline__ int run_length(const u32 *__restrict__ tcol, int stri
 
 // Runs up to n steps.  Returns kEvRun when n is used up, else the event that
 // stopped it; the lane is then exactly at the reference's state for that event.
+// hb and tgt are the low 32 bits of the reference's hashes (Lane); kEvStage
+// means they match, and stage_check decides on the full 64 bits.  keyb holds
+// the low key halves (KeyTabs::lo).
 // The stage test of the current configuration has already been done on entry
 // (re-running it at the same configuration changes nothing, as the reference
 // notes at src/e13search.c:131-133).
 //
 // Run skip: on a self-loop cell the next k steps read the same symbol, write
-// nothing and keep the state, so hb stays the same; when hb != TGT[nt] no stage
-// test can fire inside the run.  k is clamped so that every skipped step would
+// nothing and keep the state, so hb stays the same; when (the low half of) hb
+// differs from TGT[nt] no stage test can fire inside the run.  k is clamped so that every skipped step would
 // also have passed the deadline test (t + i <= deadline) and the window test
 // (the head stays in 1..1362); the step that fails either test is then taken by
 // the normal loop.  Steps counted and the death point equal single-stepping.
