@@ -211,10 +211,11 @@ __device__ __forceinline__ int run_length(const u32 *__restrict__ tcol, int stri
 //
 // Run skip: on a self-loop cell the next k steps read the same symbol, write
 // nothing and keep the state, so hb stays the same; when (the low half of) hb
-// differs from TGT[nt] no stage test can fire inside the run.  k is clamped so that every skipped step would
-// also have passed the deadline test (t + i <= deadline) and the window test
-// (the head stays in 1..1362); the step that fails either test is then taken by
-// the normal loop.  Steps counted and the death point equal single-stepping.
+// differs from TGT[nt] no stage test can fire inside the run.  k is clamped so
+// that every skipped step would also have passed the deadline test
+// (t + i <= deadline) and the window test (the head stays in 1..1362); the step
+// that fails either test is then taken by the normal loop.  Steps counted and
+// the death point equal single-stepping.
 __device__ __forceinline__ int step_slice(int &p, int &st, int &t, const int deadline, u32 &hb, const u32 tgt,
                                           u32 *__restrict__ tcol, const u32 *__restrict__ rcol,
                                           const u32 *__restrict__ keyb, const int stride, int &n, int &cell) {
