@@ -327,7 +327,8 @@ def roofline(steps, seconds, sm_mhz, nsm):
 
 
 def serve_tuning(E, tuned, stack_nodes=0):
-    """The headline's serve session: the autotuned launch shape, 200 ms epochs."""
+    """The headline's serve session: the library defaults or the autotuned
+    launch shape (tuned), 200 ms epochs."""
     t = E.tuning(epoch_us=200000, stack_nodes=stack_nodes)
     if tuned is not None:
         t.block, t.slice, t.warp_stack, t.pool_low_pct = tuned.block, tuned.slice, tuned.warp_stack, tuned.pool_low_pct
@@ -373,9 +374,10 @@ def run_sequential(E, ctx, jobs, kernel, tuned=None):
 
 def kernel_comparison(E, torch, ctx, flush, local, nsm, tuned):
     """Persistent vs plain on the same searches, both run the same way: each
-    job of the workload alone, one after another, with the same autotuned
-    block size and slice (warp stack and pool threshold exist only in the
-    persistent kernel)."""
+    job of the workload alone, one after another, with the headline's block
+    size and slice (tuned: the autotuned shape when the headline chose it,
+    else None for the library defaults; warp stack, pool threshold and the
+    run-skip age exist only in the persistent kernel)."""
     out = {}
     for name in ("local_edits_f4", "counter_sym"):
         w = WORKLOADS[name]
@@ -521,10 +523,23 @@ def main():
                       "autotune_wall_s": time.perf_counter() - t0, "block": tuned.block, "slice": tuned.slice,
                       "warp_stack": tuned.warp_stack, "pool_low_pct": tuned.pool_low_pct,
                       "run_skip": tuned.run_skip}
-    tune = serve_tuning(E, tuned, args.stack_nodes)
-
+    # warm-up: the library default and the autotuner's proposal (tuned on a
+    # proxy a quarter of the size) take turns on the whole workload, and the
+    # faster one, by its best warm-up time (the maximum over ranks), is timed
+    cands = {"default": serve_tuning(E, None, args.stack_nodes)}
+    if tuned is not None:
+        cands["autotuned"] = serve_tuning(E, tuned, args.stack_nodes)
+    warm = {k: float("inf") for k in cands}
     for _ in range(args.warmup):
-        run_concurrent(E, ctx, jobs, tune, rank, ws)
+        for k, t in cands.items():
+            warm[k] = min(warm[k], run_concurrent(E, ctx, jobs, t, rank, ws)[2])
+    if pg:
+        _, warm = S.reduce_totals(pg, {}, warm, device=f"cuda:{local}")
+    chosen = min(warm, key=lambda k: (warm[k], k != "default"))
+    tune = cands[chosen]
+    tuning_cfg.update({"chosen": chosen, "warmup_best_ms": warm, "slice_used": tune.slice, "block_used": tune.block,
+                       "warp_stack_used": tune.warp_stack, "pool_low_pct_used": tune.pool_low_pct,
+                       "run_skip_used": tune.run_skip})
     torch.cuda.synchronize()
     tot = dict(steps=0, leaves=0, dev_ms=0.0, wall=0.0, launches=0, h2d=0, d2h=0)
     per_all, lines_all = {}, []
@@ -579,7 +594,7 @@ def main():
                     "note": "host clock around the C-ABI serve calls (create, submit, step until done, destroy)"},
             "gpu_launches": tot["launches"], "clocks": clocks}
     if rank == 0 and ws == 1 and not args.no_extras:
-        line["kernels"] = kernel_comparison(E, torch, ctx, flush, local, nsm, tuned)
+        line["kernels"] = kernel_comparison(E, torch, ctx, flush, local, nsm, tuned if chosen == "autotuned" else None)
         stream = serving_mix(E, ctx)
         serving_stats(E, ctx, stream)  # warm-up of the stream's job shapes
         line["serving"] = serving_stats(E, ctx, stream)
