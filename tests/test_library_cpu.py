@@ -293,6 +293,10 @@ def test_tuning_ranges_are_checked():
     assert r == 0 and t.kernel == E.KERNEL_PERSISTENT and t.epoch_us == 10000
     r, t = E.resolve_tuning(E.tuning(slice=9, block=256))
     assert r == 0 and t.slice == 9 and t.block == 256
+    # run_skip is taken as given: 0 never, 1 always, N >= 2 from a machine age of N steps
+    for rs in (0, 1, 2, 4096, 1 << 30):
+        r, t = E.resolve_tuning(E.tuning(run_skip=rs))
+        assert r == 0 and t.run_skip == rs
     bad = [dict(epoch_us=-1), dict(epochs_per_graph=-1), dict(pool_low_pct=-5), dict(pool_low_pct=101),
            dict(block=48), dict(block=800), dict(block=100), dict(slice=-1), dict(slice=5000),
            dict(warp_stack=-2), dict(warp_stack=5000), dict(epochs_per_graph=65), dict(epoch_us=60_000_001),
