@@ -263,10 +263,12 @@ __device__ __forceinline__ int step_slice(int &p, int &st, int &t, const int dea
 }
 
 // One action of a running lane, the unit of the warp's lock-step loop: one
-// step, one run skip (SKIP only), one stage test or one first-read event.  Every running
-// lane of a warp takes exactly one action per iteration, so the warp stays
+// step, one run skip (SKIP only) or one first-read event.  Every running lane
+// of a warp takes exactly one action per iteration, so the warp stays
 // converged except inside the rare branches, which rejoin at the end of the
-// iteration.  Returns 0 (go on), kEvDead, kEvSurv or kEvCell (a cell whose
+// iteration.  Returns 0 (go on), kEvDead, kEvStage (the low hash halves match
+// after the step: the caller runs stage_check, the reference's test at the
+// start of the next step, before any further action) or kEvCell (a cell whose
 // entry has kEntSpecial; *cell and *ecell say which).  Same semantics as
 // step_slice(): each step follows src/e13search.c:134-177 in order.
 __device__ __forceinline__ int stage_check(struct Lane &L, const u32 *tcol, const KeyTabs &K, int stride);
@@ -319,7 +321,7 @@ __device__ __forceinline__ int lane_act(Lane &L, u32 *__restrict__ tcol, const u
   L.p = np;
   L.st = (int)((e >> 2) & 15u);
   L.t += k;
-  if (L.hb == L.tgt) return stage_check(L, tcol, K, stride);
+  if (L.hb == L.tgt) return kEvStage;  // the caller runs stage_check before the next action
   return 0;
 }
 

@@ -55,7 +55,8 @@ __device__ __forceinline__ void run_to_event(Lane &L, int &status, int &fork_cel
     if (status == kPrRun) {
       int cell = 0;
       u32 e = 0;
-      const int ev = lane_act<true>(L, tcol, rcol, K, stride, cell, e);
+      int ev = lane_act<true>(L, tcol, rcol, K, stride, cell, e);
+      if (ev == kEvStage) ev = stage_check(L, tcol, K, stride);
       if (ev == kEvCell) {
         if (e == kEntHalt) {
           status = kPrDead;  // a fixed halt cell

@@ -581,6 +581,10 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
               ev = lane_act<false>(L, tcol, rcol, K, stride, cell, e);
               if (!ev) ev = lane_act<false>(L, tcol, rcol, K, stride, cell, e);
             }
+            // the stage test of a hash match, once per iteration outside
+            // lane_act: one copy of it in the loop instead of one per
+            // inlined action (the second action waits for it)
+            if (ev == kEvStage) ev = stage_check(L, tcol, K, stride);
             if (ev == kEvCell) {
               if (e == kEntHalt) {
                 ev = kEvDead;
