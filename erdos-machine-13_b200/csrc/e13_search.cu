@@ -566,13 +566,10 @@ __global__ void __launch_bounds__(768, 1) search_kernel(const Params P) {
             int ev;
             if (lone_w) {
               // the same steps and events as lane_act (step_slice follows
-              // src/e13search.c:134-177 too), the stage test between steps
+              // src/e13search.c:134-177 too); a hash match ends the iteration
+              // and goes to the one stage test below
               int n = kLoneSteps;
               ev = step_slice(L.p, L.st, L.t, L.deadline, L.hb, L.tgt, tcol, rcol, K.lo, stride, n, cell);
-              while (ev == kEvStage) {
-                ev = stage_check(L, tcol, K, stride);
-                if (ev == 0 && n > 0) ev = step_slice(L.p, L.st, L.t, L.deadline, L.hb, L.tgt, tcol, rcol, K.lo, stride, n, cell);
-              }
               if (ev == kEvCell) e = get_entry(rcol, stride, cell);
             } else if (skip_w) {
               ev = lane_act<true>(L, tcol, rcol, K, stride, cell, e);
